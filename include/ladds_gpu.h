@@ -1,0 +1,233 @@
+/*
+ * ladds_gpu.h -- C ABI of the B200 (sm_100a) implementation of the LADDS
+ * per-step hot path: Yoshida-4 propagation under the OrbitPropagator
+ * acceleration set, and the linked-cell conjunction search with linear
+ * closest-approach interpolation.
+ *
+ * Plain C types only.  Every call returns an int status (LADDS_OK == 0);
+ * ladds_gpu_last_error() gives the text of the last failure.  No exception
+ * crosses this boundary.  A context is single-threaded, owns all device
+ * memory and one CUDA stream; host arrays passed in are copied.
+ *
+ * Reference interfaces replaced (paths inside the esa/LADDS tree):
+ *   - YoshidaIntegrator<AutoPas_t>(autopas, accumulator, deltaT) and
+ *     integrate(bool)                 src/ladds/Simulation.cpp:122-148, :297
+ *   - AccelerationAccumulator(std::array<bool,8> mask, ...)
+ *                                     src/ladds/Simulation.cpp:127-143
+ *   - CollisionFunctor(cutoff, dt, collisionDistanceFactor,
+ *     minDetectionRadius, evasionTrackingCutoffInKM) driven by
+ *     AutoPas::iteratePairwise(&functor) src/ladds/CollisionFunctor.h:22-89,
+ *                                     src/ladds/Simulation.cpp:211-222
+ *   - the Particle attribute set     src/ladds/particle/Particle.h:139-195
+ *   - Simulation::deleteBurnUps       src/ladds/Simulation.cpp:561-596
+ *   - Simulation::removeParticleSpawnProtection src/ladds/Simulation.cpp:470-473
+ */
+#ifndef LADDS_GPU_H
+#define LADDS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LADDS_GPU_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define LADDS_OK 0
+#define LADDS_ERR_INVALID_ARG 1 /* bad pointer, size, value or non-finite input     */
+#define LADDS_ERR_CUDA 2        /* a CUDA runtime call failed                        */
+#define LADDS_ERR_CAPACITY 3    /* caller's output buffer too small; *nOut = needed  */
+#define LADDS_ERR_NONFINITE 4   /* a state became NaN/Inf on the device              */
+#define LADDS_ERR_NO_DEVICE 5   /* no usable sm_100 device                           */
+#define LADDS_ERR_DEVICE_CHECK 6 /* a device-side bounds / wait check tripped        */
+#define LADDS_ERR_ALLOC 7       /* device or host allocation failed                  */
+#define LADDS_ERR_STATE 8       /* call not valid in the context's current state     */
+
+/* ---- propagator components: bits 0..7 follow the reference's
+ *      std::array<bool,8> order (Simulation.cpp:127-135); J3 is new. ---- */
+#define LADDS_PROP_KEP (1u << 0)
+#define LADDS_PROP_J2 (1u << 1)
+#define LADDS_PROP_C22 (1u << 2)
+#define LADDS_PROP_S22 (1u << 3)
+#define LADDS_PROP_SOL (1u << 4)
+#define LADDS_PROP_LUN (1u << 5)
+#define LADDS_PROP_SRP (1u << 6)
+#define LADDS_PROP_DRAG (1u << 7)
+#define LADDS_PROP_J3 (1u << 8)
+#define LADDS_PROP_ALL 0x1FFu
+
+/* ---- activity states: Particle::ActivityState values (Particle.h:37-53) ---- */
+#define LADDS_PASSIVE 0
+#define LADDS_EVASIVE 1
+#define LADDS_EVASIVE_PRESERVING 2
+
+/* ---- arithmetic of the propagation ---- */
+#define LADDS_PRECISION_FP64 0  /* every term in binary64                          */
+#define LADDS_PRECISION_SPLIT 1 /* central + J2 + Yoshida accumulation in binary64,
+                                   J3, C22/S22, Sun, Moon, SRP, drag in binary32  */
+
+/* ---- pair record flags ---- */
+#define LADDS_PAIR_COLLISION (1u << 0)        /* reference collision list (CollisionFunctor.cpp:112) */
+#define LADDS_PAIR_EVASION (1u << 1)          /* reference evasion list (CollisionFunctor.cpp:90)    */
+#define LADDS_PAIR_CONJUNCTION (1u << 2)      /* dl2 <= conjunctionThreshold^2, all gated pairs      */
+#define LADDS_PAIR_NEAR_COLLISION (1u << 3)   /* |dl2 - sep^2| <= nearThresholdRel * sep^2           */
+#define LADDS_PAIR_NEAR_EVASION (1u << 4)     /* same band around evasionCutoff^2                    */
+#define LADDS_PAIR_NEAR_CONJUNCTION (1u << 5) /* same band around conjunctionThreshold^2             */
+#define LADDS_PAIR_NEAR_GATE (1u << 6)        /* |d2 - cutoff^2| <= nearThresholdRel * cutoff^2      */
+
+/* One conjunction record (64 bytes).  A is the lower-id particle (lower slot on
+ * equal ids), B the other; point = p_B(t*) + 0.5 * (p_A(t*) - p_B(t*)),
+ * i.e. CollisionFunctor.cpp:94 with the reference's j = B.  Records of one call
+ * are sorted by (step, idA, idB, slotA, slotB). */
+typedef struct {
+  uint64_t idA, idB;     /* Particle::getID()                                  */
+  uint32_t slotA, slotB; /* upload index of each particle in the context       */
+  double dl2;            /* squared interpolated closest-approach distance [km^2] */
+  double point[3];       /* collision point [km]                               */
+  uint32_t step;         /* iteration index of the scan                        */
+  uint32_t flags;        /* LADDS_PAIR_* bits                                  */
+} ladds_pair;
+
+typedef struct {
+  double deltaT;                  /* sim/deltaT [s]                                    */
+  uint32_t componentMask;         /* LADDS_PROP_* bits (sim/prop/use*Component)        */
+  double epochJD;                 /* sim/referenceTime as a Julian date (UTC ~ TT)     */
+  double startTime;               /* seconds since the epoch at iteration 0            */
+  double cutoff;                  /* autopas/cutoff [km]                               */
+  double collisionDistanceFactor; /* sim/collisionDistanceFactor                       */
+  double minDetectionRadius;      /* sim/minDetectionRadius [m]                        */
+  double evasionCutoff;           /* sim/evasionTrackingCutoffInKM [km]                */
+  double conjunctionThreshold;    /* sim/conjunctionThresholdInKM [km] (new list)      */
+  double nearThresholdRel;        /* relative band of the near-threshold flags         */
+  int32_t precision;              /* LADDS_PRECISION_*                                 */
+  int32_t timestepsPerCollisionDetection; /* sim/timestepsPerCollisionDetection (k)    */
+  double cellSize;                /* cell edge [km]; <= 0 means = cutoff               */
+  double boxMin[3], boxMax[3];    /* cell-grid box [km]; objects outside are clamped   */
+  int32_t device;                 /* CUDA device ordinal                               */
+  int32_t propagateBlock;         /* threads per block of the propagation kernel (0: 256) */
+  int32_t scanBlock;              /* threads per block of the pair scan (0: 128)       */
+  int32_t useGraphs;              /* capture multi-iteration calls in CUDA graphs      */
+  uint64_t pairCapacity;          /* initial device pair-buffer capacity (0: auto)     */
+} ladds_gpu_config;
+
+typedef struct ladds_gpu_ctx ladds_gpu_ctx;
+
+/* Per-call statistics of ladds_gpu_step (device time from CUDA events). */
+typedef struct {
+  uint64_t iterations;      /* iterations run by the call                   */
+  uint64_t scans;           /* conjunction scans run by the call            */
+  uint64_t records;         /* records emitted (all flags)                  */
+  uint64_t collisions;      /* records with LADDS_PAIR_COLLISION            */
+  uint64_t evasions;        /* records with LADDS_PAIR_EVASION              */
+  uint64_t conjunctions;    /* records with LADDS_PAIR_CONJUNCTION          */
+  uint64_t retries;         /* batches re-run after a pair-buffer overflow  */
+  double deviceMs;          /* device time of the call's GPU work           */
+} ladds_step_stats;
+
+/* Fills *cfg with the reference defaults (cfg/default_cfg.yaml,
+ * Simulation.cpp:233-247): dt 10 s, KEP+J2+C22+S22+SRP+DRAG, epoch
+ * 2022-01-01, cutoff 80 km, factor 1, minDetectionRadius 0.05 m, evasion
+ * cutoff 0.1 km, conjunction threshold 0.1 km, k = 1, box +-10000 km, FP64. */
+void ladds_gpu_config_default(ladds_gpu_config *cfg);
+
+int ladds_gpu_create(const ladds_gpu_config *cfg, ladds_gpu_ctx **out);
+int ladds_gpu_destroy(ladds_gpu_ctx *ctx);
+const char *ladds_gpu_last_error(const ladds_gpu_ctx *ctx);
+int ladds_gpu_abi_version(void);
+
+/* Replaces the population.  Arrays are SoA of length n (Particle.h:139-195):
+ * position [km], velocity [km/s], radius [m], aom = pi r^2 1e-6 / m
+ * [km^2/kg] (Particle.h:72), bcInv [m^2/kg] (Particle.cpp:13-27), id,
+ * parentId (SIZE_MAX = none) and activity (LADDS_PASSIVE...).  parentId and
+ * activity may be NULL (SIZE_MAX / passive).  Slots are 0..n-1 in array order. */
+int ladds_gpu_upload(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
+                     const double *vx, const double *vy, const double *vz, const double *radius, const double *aom,
+                     const double *bcInv, const uint64_t *id, const uint64_t *parentId, const int8_t *activity);
+/* Appends particles (fragments of a breakup); they get the next slots. */
+int ladds_gpu_append(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
+                     const double *vx, const double *vy, const double *vz, const double *radius, const double *aom,
+                     const double *bcInv, const uint64_t *id, const uint64_t *parentId, const int8_t *activity);
+/* Copies the population back in slot order.  Any array pointer may be NULL. */
+int ladds_gpu_download(ladds_gpu_ctx *ctx, size_t cap, size_t *n, double *x, double *y, double *z, double *vx,
+                       double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
+                       uint64_t *parentId, int8_t *activity);
+/* Uploads / downloads only positions and velocities, in slot order (the
+ * host-owned-container mode of the drop-in). */
+int ladds_gpu_set_state(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
+                        const double *vx, const double *vy, const double *vz);
+int ladds_gpu_get_state(ladds_gpu_ctx *ctx, size_t n, double *x, double *y, double *z, double *vx, double *vy,
+                        double *vz);
+int ladds_gpu_size(const ladds_gpu_ctx *ctx, size_t *n);
+int ladds_gpu_iteration(const ladds_gpu_ctx *ctx, int64_t *iteration);
+int ladds_gpu_set_iteration(ladds_gpu_ctx *ctx, int64_t iteration);
+
+/* Replaces YoshidaIntegrator::integrate(false) (Simulation.cpp:297): `steps`
+ * Yoshida-4 steps of every particle.  Advances the iteration counter. */
+int ladds_gpu_integrate(ladds_gpu_ctx *ctx, int steps);
+
+/* Replaces collisionDetection() (Simulation.cpp:211-222) on the current
+ * state with interpolation window dtScan.  Writes up to cap records to out;
+ * *nOut = number of records.  If cap is too small returns LADDS_ERR_CAPACITY
+ * with *nOut = the number needed (nothing is lost; call again).  The three
+ * counts may be NULL. */
+int ladds_gpu_conjunctions(ladds_gpu_ctx *ctx, double dtScan, ladds_pair *out, size_t cap, size_t *nOut,
+                           size_t *nCollisions, size_t *nEvasions, size_t *nConjunctions);
+
+/* Runs `iterations` iterations of the reference loop (Simulation.cpp:287-415):
+ * integrate one step, then, when iteration % k == 0, scan with dt*k.  Records
+ * of all scans are written to out (sorted).  LADDS_ERR_CAPACITY: *nOut is the
+ * number needed; the context has then NOT advanced (re-call with a larger
+ * buffer).  stats may be NULL. */
+int ladds_gpu_step(ladds_gpu_ctx *ctx, int iterations, ladds_pair *out, size_t cap, size_t *nOut,
+                   ladds_step_stats *stats);
+
+/* Deletes particles with |r| < R_EARTH + minAltitude (Simulation.cpp:561-596);
+ * survivors keep their relative slot order and are renumbered 0..n'-1.
+ * removedIds (may be NULL) receives up to cap ids of removed particles. */
+int ladds_gpu_remove_below(ladds_gpu_ctx *ctx, double minAltitude, size_t *nRemoved, uint64_t *removedIds,
+                           size_t cap);
+/* Marks particles (by slot) as deleted: they are skipped by propagation and
+ * scans (the dummy ownership state of Simulation.cpp:368-371). */
+int ladds_gpu_mark_deleted(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t n);
+/* Sets every parentId to SIZE_MAX (Simulation.cpp:470-473). */
+int ladds_gpu_clear_parents(ladds_gpu_ctx *ctx);
+
+/* Cell order of the last scan: for each sorted position its cell key and slot.
+ * Used to check the sort order bit-exactly against a CPU restatement. */
+int ladds_gpu_cell_order(ladds_gpu_ctx *ctx, size_t cap, size_t *n, uint32_t *keys, uint32_t *slots);
+/* Grid actually used: cells per dimension, reach and cell size. */
+int ladds_gpu_grid(const ladds_gpu_ctx *ctx, int32_t dims[3], int32_t *reach, double *cellSize);
+
+/* Device time of the kernels of the last call, per phase [ms]: propagate,
+ * sort (keys + radix passes), cell table (permute + row starts), pair scan. */
+typedef struct {
+  double propagateMs, sortMs, cellMs, scanMs, totalMs;
+  uint64_t propagateLaunches, sortLaunches, cellLaunches, scanLaunches;
+} ladds_phase_times;
+int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
+int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
+
+/* ---- synthetic populations (host) ---- */
+/* Fills SoA arrays with population `which` of the benchmark definitions:
+ *  0: N objects, a = R + U[400,1500] km, e U[0,0.02], i U[0,180] deg, RAAN /
+ *     argp / M U[0,2pi), radius logU[0.01,5] m, rho 2700 kg/m^3, Cd 2.2;
+ *  2: the four constellation shells (4224 evasive satellites) followed by
+ *     N - 4224 objects of population 0;
+ *  4: N - 500000 small debris (radius logU[0.01,0.1] m, altitude from
+ *     0.5 N(800,60) + 0.5 N(1450,80) truncated to [300,2000] km) followed by
+ *     500000 objects of population 0 (fewer when N < 500000).
+ * Element draw of object k uses its own splitmix64 -> xoshiro256** stream
+ * seeded from (seed, k), so any slice is reproducible on its own. */
+int ladds_population_generate(int which, uint64_t seed, size_t n, double *x, double *y, double *z, double *vx,
+                              double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
+                              uint64_t *parentId, int8_t *activity);
+/* Keplerian elements -> Cartesian state (km, km/s), Kepler's equation by Newton. */
+int ladds_elements_to_state(double a, double e, double inc, double raan, double argp, double meanAnomaly,
+                            double r[3], double v[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

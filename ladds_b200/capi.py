@@ -1,0 +1,344 @@
+"""ctypes binding of ``libladds_gpu.so`` (the C ABI in ``include/ladds_gpu.h``).
+
+This is the Python face of the library used by the tests and the benchmark;
+the C++ host mirror of the reference interface lives in ``ladds_b200/host``.
+The shared library is built in-tree by ``ladds_b200.build``; if it is missing
+the import fails loudly -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libladds_gpu.so")
+
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_CAPACITY, ERR_NONFINITE, ERR_NO_DEVICE, ERR_DEVICE_CHECK, ERR_ALLOC, ERR_STATE = \
+    range(9)
+KEP, J2, C22, S22, SOL, LUN, SRP, DRAG, J3 = (1 << k for k in range(9))
+PROP_ALL = 0x1FF
+PASSIVE, EVASIVE, EVASIVE_PRESERVING = 0, 1, 2
+PRECISION_FP64, PRECISION_SPLIT = 0, 1
+PAIR_COLLISION, PAIR_EVASION, PAIR_CONJUNCTION = 1, 2, 4
+PAIR_NEAR_COLLISION, PAIR_NEAR_EVASION, PAIR_NEAR_CONJUNCTION, PAIR_NEAR_GATE = 8, 16, 32, 64
+SIZE_MAX = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+PAIR_DTYPE = np.dtype([("idA", "<u8"), ("idB", "<u8"), ("slotA", "<u4"), ("slotB", "<u4"), ("dl2", "<f8"),
+                       ("point", "<f8", (3,)), ("step", "<u4"), ("flags", "<u4")])
+assert PAIR_DTYPE.itemsize == 64
+
+
+class LaddsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"ladds_gpu error {code}: {msg}")
+        self.code = code
+
+
+class GpuConfig(C.Structure):
+    _fields_ = [
+        ("deltaT", C.c_double),
+        ("componentMask", C.c_uint32),
+        ("epochJD", C.c_double),
+        ("startTime", C.c_double),
+        ("cutoff", C.c_double),
+        ("collisionDistanceFactor", C.c_double),
+        ("minDetectionRadius", C.c_double),
+        ("evasionCutoff", C.c_double),
+        ("conjunctionThreshold", C.c_double),
+        ("nearThresholdRel", C.c_double),
+        ("precision", C.c_int32),
+        ("timestepsPerCollisionDetection", C.c_int32),
+        ("cellSize", C.c_double),
+        ("boxMin", C.c_double * 3),
+        ("boxMax", C.c_double * 3),
+        ("device", C.c_int32),
+        ("propagateBlock", C.c_int32),
+        ("scanBlock", C.c_int32),
+        ("useGraphs", C.c_int32),
+        ("pairCapacity", C.c_uint64),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("scans", C.c_uint64), ("records", C.c_uint64),
+                ("collisions", C.c_uint64), ("evasions", C.c_uint64), ("conjunctions", C.c_uint64),
+                ("retries", C.c_uint64), ("deviceMs", C.c_double)]
+
+
+class PhaseTimes(C.Structure):
+    _fields_ = [("propagateMs", C.c_double), ("sortMs", C.c_double), ("cellMs", C.c_double), ("scanMs", C.c_double),
+                ("totalMs", C.c_double), ("propagateLaunches", C.c_uint64), ("sortLaunches", C.c_uint64),
+                ("cellLaunches", C.c_uint64), ("scanLaunches", C.c_uint64)]
+
+
+EXPORTED = [
+    "ladds_gpu_abi_version", "ladds_gpu_config_default", "ladds_gpu_create", "ladds_gpu_destroy",
+    "ladds_gpu_last_error", "ladds_gpu_upload", "ladds_gpu_append", "ladds_gpu_download", "ladds_gpu_set_state",
+    "ladds_gpu_get_state", "ladds_gpu_size", "ladds_gpu_iteration", "ladds_gpu_set_iteration",
+    "ladds_gpu_integrate", "ladds_gpu_conjunctions", "ladds_gpu_step", "ladds_gpu_remove_below",
+    "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
+    "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
+]
+
+_lib = None
+
+
+def lib():
+    """Loads the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m ladds_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, sz, i = C.c_void_p, C.c_size_t, C.c_int
+    L.ladds_gpu_abi_version.restype = i
+    L.ladds_gpu_config_default.argtypes = [C.POINTER(GpuConfig)]
+    L.ladds_gpu_create.argtypes = [C.POINTER(GpuConfig), C.POINTER(vp)]
+    L.ladds_gpu_destroy.argtypes = [vp]
+    L.ladds_gpu_last_error.restype = C.c_char_p
+    L.ladds_gpu_last_error.argtypes = [vp]
+    L.ladds_gpu_upload.argtypes = [vp, sz] + [vp] * 12
+    L.ladds_gpu_append.argtypes = [vp, sz] + [vp] * 12
+    L.ladds_gpu_download.argtypes = [vp, sz, C.POINTER(sz)] + [vp] * 12
+    L.ladds_gpu_set_state.argtypes = [vp, sz] + [vp] * 6
+    L.ladds_gpu_get_state.argtypes = [vp, sz] + [vp] * 6
+    L.ladds_gpu_size.argtypes = [vp, C.POINTER(sz)]
+    L.ladds_gpu_iteration.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.ladds_gpu_set_iteration.argtypes = [vp, C.c_int64]
+    L.ladds_gpu_integrate.argtypes = [vp, i]
+    L.ladds_gpu_conjunctions.argtypes = [vp, C.c_double, vp, sz, C.POINTER(sz), C.POINTER(sz), C.POINTER(sz),
+                                         C.POINTER(sz)]
+    L.ladds_gpu_step.argtypes = [vp, i, vp, sz, C.POINTER(sz), C.POINTER(StepStats)]
+    L.ladds_gpu_remove_below.argtypes = [vp, C.c_double, C.POINTER(sz), vp, sz]
+    L.ladds_gpu_mark_deleted.argtypes = [vp, vp, sz]
+    L.ladds_gpu_clear_parents.argtypes = [vp]
+    L.ladds_gpu_cell_order.argtypes = [vp, sz, C.POINTER(sz), vp, vp]
+    L.ladds_gpu_grid.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.ladds_gpu_phase_times.argtypes = [vp, C.POINTER(PhaseTimes)]
+    L.ladds_gpu_set_profiling.argtypes = [vp, i]
+    L.ladds_population_generate.argtypes = [i, C.c_uint64, sz] + [vp] * 12
+    L.ladds_elements_to_state.argtypes = [C.c_double] * 6 + [vp, vp]
+    _lib = L
+    return L
+
+
+def default_config(**overrides) -> GpuConfig:
+    cfg = GpuConfig()
+    lib().ladds_gpu_config_default(C.byref(cfg))
+    for k, v in overrides.items():
+        if k in ("boxMin", "boxMax"):
+            getattr(cfg, k)[:] = list(v)
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+POP_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "radius", "aom", "bc_inv", "id", "parent", "activity")
+_POP_DTYPES = dict(x=np.float64, y=np.float64, z=np.float64, vx=np.float64, vy=np.float64, vz=np.float64,
+                   radius=np.float64, aom=np.float64, bc_inv=np.float64, id=np.uint64, parent=np.uint64,
+                   activity=np.int8)
+
+
+def empty_population(n: int) -> dict:
+    return {k: np.zeros(n, dtype=t) for k, t in _POP_DTYPES.items()}
+
+
+def as_population(d: dict) -> dict:
+    out = {}
+    n = len(d["x"])
+    for k, t in _POP_DTYPES.items():
+        if k in d and d[k] is not None:
+            out[k] = np.ascontiguousarray(d[k], dtype=t)
+        elif k == "parent":
+            out[k] = np.full(n, SIZE_MAX, dtype=np.uint64)
+        elif k == "activity":
+            out[k] = np.zeros(n, dtype=np.int8)
+        elif k == "id":
+            out[k] = np.arange(n, dtype=np.uint64)
+        else:
+            raise KeyError(k)
+    return out
+
+
+def generate_population(which: int, seed: int, n: int) -> dict:
+    pop = empty_population(n)
+    rc = lib().ladds_population_generate(which, seed, n, *[_p(pop[k]) for k in POP_FIELDS])
+    if rc:
+        raise LaddsError(rc, "population generation failed")
+    return pop
+
+
+def elements_to_state(a, e, inc, raan, argp, M):
+    r = np.zeros(3)
+    v = np.zeros(3)
+    rc = lib().ladds_elements_to_state(a, e, inc, raan, argp, M, _p(r), _p(v))
+    if rc:
+        raise LaddsError(rc, "bad elements")
+    return r, v
+
+
+@dataclass
+class StepResult:
+    records: np.ndarray
+    stats: StepStats
+
+
+class Context:
+    """One device context (``ladds_gpu_ctx``)."""
+
+    def __init__(self, config: GpuConfig | None = None, **overrides):
+        self._L = lib()
+        cfg = config if config is not None else default_config()
+        for k, v in overrides.items():
+            if k in ("boxMin", "boxMax"):
+                getattr(cfg, k)[:] = list(v)
+            else:
+                setattr(cfg, k, v)
+        self.config = cfg
+        h = C.c_void_p()
+        rc = self._L.ladds_gpu_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise LaddsError(rc, "ladds_gpu_create failed")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ladds_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            msg = self._L.ladds_gpu_last_error(self._h)
+            raise LaddsError(rc, msg.decode() if msg else "")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, pop: dict):
+        pop = as_population(pop)
+        self._keep = pop
+        self._check(self._L.ladds_gpu_upload(self._h, len(pop["x"]), *[_p(pop[k]) for k in POP_FIELDS]))
+
+    def append(self, pop: dict):
+        pop = as_population(pop)
+        self._check(self._L.ladds_gpu_append(self._h, len(pop["x"]), *[_p(pop[k]) for k in POP_FIELDS]))
+
+    def size(self) -> int:
+        n = C.c_size_t()
+        self._check(self._L.ladds_gpu_size(self._h, C.byref(n)))
+        return n.value
+
+    def iteration(self) -> int:
+        it = C.c_int64()
+        self._check(self._L.ladds_gpu_iteration(self._h, C.byref(it)))
+        return it.value
+
+    def set_iteration(self, it: int):
+        self._check(self._L.ladds_gpu_set_iteration(self._h, it))
+
+    def download(self) -> dict:
+        n = self.size()
+        pop = empty_population(n)
+        got = C.c_size_t()
+        self._check(self._L.ladds_gpu_download(self._h, n, C.byref(got), *[_p(pop[k]) for k in POP_FIELDS]))
+        return pop
+
+    def set_state(self, x, y, z, vx, vy, vz):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, vx, vy, vz)]
+        self._check(self._L.ladds_gpu_set_state(self._h, len(arrs[0]), *[_p(a) for a in arrs]))
+
+    def get_state(self):
+        n = self.size()
+        arrs = [np.zeros(n) for _ in range(6)]
+        self._check(self._L.ladds_gpu_get_state(self._h, n, *[_p(a) for a in arrs]))
+        return arrs
+
+    def integrate(self, steps: int):
+        self._check(self._L.ladds_gpu_integrate(self._h, steps))
+
+    def conjunctions(self, dt_scan: float, cap: int | None = None):
+        cap = 4096 if cap is None else cap
+        while True:
+            out = np.zeros(max(cap, 1), dtype=PAIR_DTYPE)
+            n, nc, ne, nj = C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_size_t()
+            rc = self._L.ladds_gpu_conjunctions(self._h, dt_scan, _p(out), cap, C.byref(n), C.byref(nc),
+                                                C.byref(ne), C.byref(nj))
+            if rc == ERR_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return out[: n.value].copy()
+
+    def step(self, iterations: int, cap: int | None = None, out: np.ndarray | None = None) -> StepResult:
+        if out is not None:
+            cap = len(out)
+        cap = 4096 if cap is None else cap
+        while True:
+            buf = out if (out is not None and len(out) >= cap) else np.zeros(max(cap, 1), dtype=PAIR_DTYPE)
+            n = C.c_size_t()
+            st = StepStats()
+            rc = self._L.ladds_gpu_step(self._h, iterations, _p(buf), cap, C.byref(n), C.byref(st))
+            if rc == ERR_CAPACITY and n.value > cap:
+                cap = n.value
+                out = None
+                continue
+            self._check(rc)
+            return StepResult(buf[: n.value].copy(), st)
+
+    def cell_order(self):
+        n = self.size()
+        keys = np.zeros(n, dtype=np.uint32)
+        slots = np.zeros(n, dtype=np.uint32)
+        got = C.c_size_t()
+        self._check(self._L.ladds_gpu_cell_order(self._h, n, C.byref(got), _p(keys), _p(slots)))
+        return keys, slots
+
+    def grid(self):
+        dims = (C.c_int32 * 3)()
+        reach = C.c_int32()
+        cell = C.c_double()
+        self._check(self._L.ladds_gpu_grid(self._h, dims, C.byref(reach), C.byref(cell)))
+        return tuple(dims), reach.value, cell.value
+
+    def remove_below(self, min_altitude: float):
+        n = self.size()
+        ids = np.zeros(max(n, 1), dtype=np.uint64)
+        removed = C.c_size_t()
+        self._check(self._L.ladds_gpu_remove_below(self._h, min_altitude, C.byref(removed), _p(ids), n))
+        return ids[: removed.value].copy()
+
+    def mark_deleted(self, slots):
+        slots = np.ascontiguousarray(slots, dtype=np.uint32)
+        self._check(self._L.ladds_gpu_mark_deleted(self._h, _p(slots), len(slots)))
+
+    def clear_parents(self):
+        self._check(self._L.ladds_gpu_clear_parents(self._h))
+
+    def set_profiling(self, on: bool):
+        self._check(self._L.ladds_gpu_set_profiling(self._h, 1 if on else 0))
+
+    def phase_times(self) -> PhaseTimes:
+        t = PhaseTimes()
+        self._check(self._L.ladds_gpu_phase_times(self._h, C.byref(t)))
+        return t

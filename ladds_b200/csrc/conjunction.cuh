@@ -1,0 +1,344 @@
+// conjunction.cuh -- cell table and pair scan.
+//
+// Replaces AutoPas::iteratePairwise(&CollisionFunctor) (Simulation.cpp:220,
+// external traversal) together with CollisionFunctor::AoSFunctor
+// (CollisionFunctor.cpp:40-131) and utils::distanceByLinearInterpolation
+// (DistanceApproximation.cpp:13-58).
+//
+// After the radix sort the population is gathered into cell order.  Keys are
+// row-major, (iz*ny + iy)*nx + ix, so the cells (ix-R..ix+R) of one row are a
+// contiguous key window.  rowStart[r] = first sorted index of row r.  One
+// thread per sorted object visits, like a Newton3 linked-cell traversal, each
+// neighbouring pair once: the rest of its own row window (ix..ix+R, later
+// objects only) and the rows (dz,dy) > (0,0) lexicographically, each located by
+// a binary search inside its row.  The candidate test and the functor use
+// explicitly rounded operations (__dmul_rn / __dadd_rn / __dsub_rn /
+// __ddiv_rn) in the reference's evaluation order, so results are bit-identical
+// to a binary64 CPU evaluation without FMA contraction, NaN path included.
+#pragma once
+#include "../../include/ladds_gpu.h"
+#include "physics.cuh"
+#include "state.cuh"
+
+namespace ladds {
+
+__global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n,
+                          double4 *__restrict__ pos4, unsigned *__restrict__ status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint32_t p = perm[j];
+  if (p >= (uint32_t)n) {  // a sort defect: record it and keep the access in bounds
+    atomicOr(status, 4u);
+    p = (uint32_t)j;
+  }
+  const double x = src.x[p], y = src.y[p], z = src.z[p];
+  dst.x[j] = x;
+  dst.y[j] = y;
+  dst.z[j] = z;
+  pos4[j] = make_double4(x, y, z, 0.0);  // packed copy read by the candidate test
+  dst.vx[j] = src.vx[p];
+  dst.vy[j] = src.vy[p];
+  dst.vz[j] = src.vz[p];
+  dst.aom[j] = src.aom[p];
+  dst.bc[j] = src.bc[p];
+  dst.radius[j] = src.radius[p];
+  dst.id[j] = src.id[p];
+  dst.parent[j] = src.parent[p];
+  dst.tag[j] = src.tag[p];
+}
+
+// rowStart[r] = lower_bound(skeys, r * nx), r in [0, nRows]
+__global__ void k_row_start(const uint32_t *__restrict__ skeys, int n, uint32_t nx, uint32_t nRows,
+                            uint32_t *__restrict__ rowStart) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > nRows) return;
+  const uint64_t v = (uint64_t)r * nx;
+  uint32_t lo = 0, hi = (uint32_t)n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((uint64_t)skeys[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  rowStart[r] = lo;
+}
+
+__device__ __forceinline__ double dot3rn(const double a[3], const double b[3]) {
+  double r = __dadd_rn(0.0, __dmul_rn(a[0], b[0]));
+  r = __dadd_rn(r, __dmul_rn(a[1], b[1]));
+  return __dadd_rn(r, __dmul_rn(a[2], b[2]));
+}
+
+// distanceByLinearInterpolation (DistanceApproximation.cpp:13-58)
+__device__ __forceinline__ void interpolate(const double ri[3], const double vi[3], const double rj[3],
+                                            const double vj[3], double dt, double dr[3], double p2[3]) {
+  double oi[3], oj[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    oi[k] = __dsub_rn(ri[k], __dmul_rn(vi[k], dt));
+    oj[k] = __dsub_rn(rj[k], __dmul_rn(vj[k], dt));
+  }
+  const double vi_ri = dot3rn(vi, oi), vi_rj = dot3rn(vi, oj), vj_ri = dot3rn(vj, oi), vj_rj = dot3rn(vj, oj);
+  const double num = __dsub_rn(__dsub_rn(__dadd_rn(vi_rj, vj_ri), vi_ri), vj_rj);
+  const double two = __dmul_rn(2.0, dot3rn(vi, vj));
+  const double den = __dsub_rn(__dadd_rn(dot3rn(vi, vi), dot3rn(vj, vj)), two);
+  double t = __ddiv_rn(num, den);
+  t = (t < 0.0) ? 0.0 : ((dt < t) ? dt : t);  // std::clamp: NaN passes
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double p1 = __dadd_rn(oi[k], __dmul_rn(vi[k], t));
+    p2[k] = __dadd_rn(oj[k], __dmul_rn(vj[k], t));
+    dr[k] = __dsub_rn(p1, p2[k]);
+  }
+}
+
+__device__ __forceinline__ bool nearBand(double x, double thr2, double rel) {
+  return fabs(__dsub_rn(x, thr2)) <= __dmul_rn(rel, thr2);
+}
+
+struct Obj {
+  double r[3], v[3], radius;
+  uint64_t id, parent;
+  uint32_t tag;
+};
+
+__device__ __forceinline__ void loadObj(const DevState &s, int k, Obj &o) {
+  o.r[0] = s.x[k];
+  o.r[1] = s.y[k];
+  o.r[2] = s.z[k];
+  o.v[0] = s.vx[k];
+  o.v[1] = s.vy[k];
+  o.v[2] = s.vz[k];
+  o.radius = s.radius[k];
+  o.id = s.id[k];
+  o.parent = s.parent[k];
+  o.tag = s.tag[k];
+}
+
+// CollisionFunctor::AoSFunctor on (i, j) with the gate already evaluated.
+__device__ __forceinline__ uint32_t functorPair(const ScanConsts &c, const Obj &I, const Obj &J, double d2,
+                                                double &dl2, double point[3]) {
+  const int ai = tagAct(I.tag), aj = tagAct(J.tag);
+  const bool wasEvaded = (ai != kPassive && aj != kPassive) || (ai != kPassive && J.radius >= c.minDetectionRadius) ||
+                         (aj != kPassive && I.radius >= c.minDetectionRadius);
+  if (I.parent != UINT64_MAX && I.parent == J.parent) return 0u;
+  uint32_t flags = nearBand(d2, c.cutoffSq, c.nearRel) ? LADDS_PAIR_NEAR_GATE : 0u;
+  const bool gate = !(d2 > c.cutoffSq);
+  if (!gate && !flags) return 0u;
+  double drl[3], p2[3];
+  interpolate(I.r, I.v, J.r, J.v, c.dt, drl, p2);
+  dl2 = dot3rn(drl, drl);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) point[k] = __dadd_rn(p2[k], __dmul_rn(drl[k], 0.5));
+  if (!gate) return flags;
+  if (wasEvaded) {
+    if (!(dl2 > c.evasionSq)) flags |= LADDS_PAIR_EVASION;
+    if (nearBand(dl2, c.evasionSq, c.nearRel)) flags |= LADDS_PAIR_NEAR_EVASION;
+  } else {
+    const double sep = __dmul_rn(__dadd_rn(I.radius, J.radius), c.factor);
+    const double sep2 = __dmul_rn(sep, sep);
+    if (!(dl2 > sep2)) flags |= LADDS_PAIR_COLLISION;
+    if (nearBand(dl2, sep2, c.nearRel)) flags |= LADDS_PAIR_NEAR_COLLISION;
+  }
+  if (!(dl2 > c.conjSq)) flags |= LADDS_PAIR_CONJUNCTION;
+  if (nearBand(dl2, c.conjSq, c.nearRel)) flags |= LADDS_PAIR_NEAR_CONJUNCTION;
+  return flags;
+}
+
+__device__ __forceinline__ uint32_t lowerBound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi, uint32_t v) {
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void emitPair(const Obj &I, const Obj &J, double dl2, const double point[3],
+                                         uint32_t flags, uint32_t step, ladds_pair *__restrict__ out,
+                                         unsigned long long *__restrict__ count, unsigned long long cap) {
+  const unsigned long long pos = atomicAdd(count, 1ull);
+  if (pos < cap) {
+    ladds_pair p;
+    p.idA = I.id;
+    p.idB = J.id;
+    p.slotA = tagSlot(I.tag);
+    p.slotB = tagSlot(J.tag);
+    p.dl2 = dl2;
+    p.point[0] = point[0];
+    p.point[1] = point[1];
+    p.point[2] = point[2];
+    p.step = step;
+    p.flags = flags;
+    out[pos] = p;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_pair_scan(DevState s, const double4 *__restrict__ pos4, int n,
+                                                   const uint32_t *__restrict__ skeys,
+                                                   const uint32_t *__restrict__ rowStart, GridDesc g, ScanConsts c,
+                                                   const int64_t *__restrict__ iterPtr, int64_t iterOffset,
+                                                   ladds_pair *__restrict__ out,
+                                                   unsigned long long *__restrict__ count, unsigned long long cap) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int64_t it = *iterPtr + iterOffset;  // iteration index stored in the records
+  const uint32_t step = it < 0 ? 0u : (uint32_t)it;
+  const uint32_t myTag = s.tag[j];
+  if (tagDummy(myTag)) return;
+  Obj me;
+  loadObj(s, j, me);
+  const uint32_t key = skeys[j];
+  const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
+  const int32_t ix = (int32_t)(key % (uint32_t)nx);
+  const uint32_t row = key / (uint32_t)nx;
+  const int32_t iy = (int32_t)(row % (uint32_t)ny), iz = (int32_t)(row / (uint32_t)ny);
+  const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
+  for (int dz = 0; dz <= R; ++dz) {
+    const int32_t jz = iz + dz;
+    if (jz >= nz) break;
+    for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
+      const int32_t jy = iy + dy;
+      if (jy < 0 || jy >= ny) continue;
+      const uint32_t r2 = (uint32_t)jz * (uint32_t)ny + (uint32_t)jy;
+      const uint32_t rowBase = r2 * (uint32_t)nx;
+      const uint32_t end = rowStart[r2 + 1];
+      uint32_t k;
+      if (dz == 0 && dy == 0)
+        k = (uint32_t)j + 1;
+      else
+        k = lowerBound(skeys, rowStart[r2], end, rowBase + xlo);
+      const uint32_t hiKey = rowBase + xhi;
+      for (; k < end; ++k) {
+        if (skeys[k] > hiKey) break;
+        const double4 q = pos4[k];
+        const double o[3] = {q.x, q.y, q.z};
+        double d[3];
+        d[0] = __dsub_rn(me.r[0], o[0]);
+        d[1] = __dsub_rn(me.r[1], o[1]);
+        d[2] = __dsub_rn(me.r[2], o[2]);
+        const double d2 = dot3rn(d, d);  // symmetric in (i, j) bit for bit
+        if (d2 > c.cutoffSq && !nearBand(d2, c.cutoffSq, c.nearRel)) continue;
+        Obj other;
+        loadObj(s, (int)k, other);
+        if (tagDummy(other.tag)) continue;
+        const bool meFirst = me.id < other.id || (me.id == other.id && tagSlot(me.tag) < tagSlot(other.tag));
+        const Obj &I = meFirst ? me : other;
+        const Obj &J = meFirst ? other : me;
+        double dl2 = 0.0, point[3] = {0.0, 0.0, 0.0};
+        const uint32_t f = functorPair(c, I, J, d2, dl2, point);
+        if (f) emitPair(I, J, dl2, point, f, step, out, count, cap);
+      }
+    }
+  }
+}
+
+// Scatter the sorted population back to slot order (download path).
+// (slots are dense in [0, n); the guards only keep a corrupted tag in bounds)
+__global__ void k_unpermute_f64(const double *__restrict__ src, const uint32_t *__restrict__ tag, int n,
+                                double *__restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = src[j];
+}
+__global__ void k_unpermute_u64(const uint64_t *__restrict__ src, const uint32_t *__restrict__ tag, int n,
+                                uint64_t *__restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = src[j];
+}
+__global__ void k_unpermute_act(const uint32_t *__restrict__ tag, int n, int8_t *__restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = (int8_t)tagAct(tag[j]);
+}
+// Gather slot-ordered values into the current (sorted) order (state upload).
+__global__ void k_permute_from_slots_f64(const double *__restrict__ src, const uint32_t *__restrict__ tag, int n,
+                                         double *__restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[j] = src[tagSlot(tag[j])];
+}
+
+__global__ void k_clear_parents(uint64_t *__restrict__ parent, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) parent[j] = UINT64_MAX;
+}
+
+// slotMark[slot] = 1 for slots to delete
+__global__ void k_mark_deleted(uint32_t *__restrict__ tag, const uint8_t *__restrict__ slotMark, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n && slotMark[tagSlot(tag[j])]) tag[j] |= kTagDummy;
+}
+
+// keep[j] = 1 if the object survives the burn-up test |r|^2 >= crit^2
+// (Simulation.cpp:581-590); aliveBySlot[slot] mirrors it in slot order.
+__global__ void k_burnup_flags(const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const uint32_t *__restrict__ tag, int n,
+                               double critSq, uint32_t *__restrict__ keep, uint32_t *__restrict__ aliveBySlot) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double a2 = x[j] * x[j] + y[j] * y[j] + z[j] * z[j];
+  const uint32_t k = (a2 < critSq) ? 0u : 1u;
+  keep[j] = k;
+  if (tagSlot(tag[j]) < (uint32_t)n) aliveBySlot[tagSlot(tag[j])] = k;
+}
+
+// compaction: dst[pos[j]] = src[j] for kept j; slots renumbered via newSlot
+__global__ void k_compact(DevState src, DevState dst, const uint32_t *__restrict__ keep,
+                          const uint32_t *__restrict__ pos, const uint32_t *__restrict__ newSlot, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || !keep[j]) return;
+  const uint32_t p = pos[j];
+  dst.x[p] = src.x[j];
+  dst.y[p] = src.y[j];
+  dst.z[p] = src.z[j];
+  dst.vx[p] = src.vx[j];
+  dst.vy[p] = src.vy[j];
+  dst.vz[p] = src.vz[j];
+  dst.aom[p] = src.aom[j];
+  dst.bc[p] = src.bc[j];
+  dst.radius[p] = src.radius[j];
+  dst.id[p] = src.id[j];
+  dst.parent[p] = src.parent[j];
+  const uint32_t t = src.tag[j];
+  const uint32_t ns = tagSlot(t) < (uint32_t)n ? newSlot[tagSlot(t)] : 0u;
+  dst.tag[p] = (t & ~kTagSlotMask) | (ns & kTagSlotMask);
+}
+
+// exclusive scan of u32 flags, three phases (block sums, scan of sums, apply)
+constexpr int kScanBlock = 1024;
+__global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const uint32_t *__restrict__ in, int n,
+                                                            uint32_t *__restrict__ out,
+                                                            uint32_t *__restrict__ blockSums) {
+  __shared__ uint32_t ws[32];
+  const int i = blockIdx.x * kScanBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t v = i < n ? in[i] : 0u;
+  uint32_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) ws[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t off = warp ? ws[warp - 1] : 0u;
+  if (i < n) out[i] = off + incl - v;
+  if (threadIdx.x == kScanBlock - 1) blockSums[blockIdx.x] = off + incl;
+}
+__global__ void k_scan_add(uint32_t *__restrict__ out, int n, const uint32_t *__restrict__ blockOffsets) {
+  const int i = blockIdx.x * kScanBlock + threadIdx.x;
+  if (i < n) out[i] += blockOffsets[blockIdx.x];
+}
+
+}  // namespace ladds

@@ -1,0 +1,201 @@
+// forces.cuh -- device acceleration set, FP64 and split precision.
+//
+// FP64:  every term in binary64 (third body in the direct difference form).
+// SPLIT: central term, J2 and the altitude used for the drag band in binary64;
+//        J3, C22/S22, Sun, Moon (Battin's f(q) form, free of the cancellation
+//        of the direct form), SRP and drag in binary32, each added to the
+//        binary64 sum.  The Yoshida drift/kick accumulation stays binary64.
+#pragma once
+#include "physics.cuh"
+
+namespace ladds {
+
+struct AtmShared {
+  double h0[kAtmBands], rho0[kAtmBands], H[kAtmBands];
+};
+
+// band index: largest k with h0[k] <= h (0 below the table)
+__device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
+  int k = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int c = k + step;
+    if (c < kAtmBands && h >= t.h0[c]) k = c;
+  }
+  return k;
+}
+
+// Battin's f(q) = (1+q)^{3/2} - 1 written without cancellation.
+__device__ __forceinline__ float battinF(float q) {
+  const float s = 1.0f + q;
+  const float s32 = s * sqrtf(s);
+  return q * (3.0f + q * (3.0f + q)) / (1.0f + s32);
+}
+
+template <bool SPLIT>
+__device__ __forceinline__ void accel(uint32_t mask, const double r[3], const double v[3], double aom, double bcInv,
+                                      const EphEntry &e, const AtmShared &atm, double a[3]) {
+  const double x = r[0], y = r[1], z = r[2];
+  const double r2 = x * x + y * y + z * z;
+  const double rinv = rsqrt(r2);
+  const double rn = r2 * rinv;
+  const double rinv2 = rinv * rinv;
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  if (mask & kPropKEP) {
+    const double k = -kMuEarth * rinv2 * rinv;
+    ax += k * x;
+    ay += k * y;
+    az += k * z;
+  }
+  if (mask & kPropJ2) {
+    const double k = (-1.5 * kJ2 * kMuEarth * kREarth * kREarth) * (rinv2 * rinv2 * rinv);
+    const double zr2 = z * z * rinv2;
+    ax += k * x * (1.0 - 5.0 * zr2);
+    ay += k * y * (1.0 - 5.0 * zr2);
+    az += k * z * (3.0 - 5.0 * zr2);
+  }
+  if constexpr (!SPLIT) {
+    if (mask & kPropJ3) {
+      const double k = (-2.5 * kJ3 * kMuEarth * kREarth * kREarth * kREarth) * (rinv2 * rinv2 * rinv2 * rinv);
+      const double z2 = z * z;
+      const double f = 3.0 * z - 7.0 * z2 * z * rinv2;
+      ax += k * x * f;
+      ay += k * y * f;
+      az += k * (6.0 * z2 - 7.0 * z2 * z2 * rinv2 - 0.6 * r2);
+    }
+    if (mask & (kPropC22 | kPropS22)) {
+      const double C = (mask & kPropC22) ? kC22 : 0.0;
+      const double S = (mask & kPropS22) ? kS22 : 0.0;
+      const double c = e.cosT, s = e.sinT;
+      const double xf = c * x + s * y, yf = -s * x + c * y;
+      const double g = C * (xf * xf - yf * yf) + 2.0 * S * xf * yf;
+      const double k = (3.0 * kMuEarth * kREarth * kREarth) * (rinv2 * rinv2 * rinv);
+      const double axf = k * (2.0 * (C * xf + S * yf) - 5.0 * g * xf * rinv2);
+      const double ayf = k * (2.0 * (S * xf - C * yf) - 5.0 * g * yf * rinv2);
+      ax += c * axf - s * ayf;
+      ay += s * axf + c * ayf;
+      az += k * (-5.0 * g * z * rinv2);
+    }
+    if (mask & kPropSOL) {
+      const double dx = e.sun[0] - x, dy = e.sun[1] - y, dz = e.sun[2] - z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double di = rsqrt(d2);
+      const double kd = kMuSun * di * di * di;
+      ax += kd * dx - e.sunK * e.sun[0];
+      ay += kd * dy - e.sunK * e.sun[1];
+      az += kd * dz - e.sunK * e.sun[2];
+    }
+    if (mask & kPropLUN) {
+      const double dx = e.moon[0] - x, dy = e.moon[1] - y, dz = e.moon[2] - z;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double di = rsqrt(d2);
+      const double kd = kMuMoon * di * di * di;
+      ax += kd * dx - e.moonK * e.moon[0];
+      ay += kd * dy - e.moonK * e.moon[1];
+      az += kd * dz - e.moonK * e.moon[2];
+    }
+    if (mask & kPropSRP) {
+      const double proj = x * e.sunHat[0] + y * e.sunHat[1] + z * e.sunHat[2];
+      const bool shadow = proj < 0.0 && (r2 - proj * proj) < kREarth * kREarth;
+      if (!shadow) {
+        const double ux = x - e.sun[0], uy = y - e.sun[1], uz = z - e.sun[2];
+        const double u2 = ux * ux + uy * uy + uz * uz;
+        const double ui = rsqrt(u2);
+        const double k = (kCR * kPSrp * kAU * kAU * 1.0e3) * aom * (ui * ui * ui);
+        ax += k * ux;
+        ay += k * uy;
+        az += k * uz;
+      }
+    }
+    if (mask & kPropDRAG) {
+      const double wx = v[0] + kOmegaEarth * y, wy = v[1] - kOmegaEarth * x, wz = v[2];
+      const double wn = sqrt(wx * wx + wy * wy + wz * wz);
+      const double h = rn - kREarth;
+      const int b = atmBand(atm, h);
+      const double rho = atm.rho0[b] * exp(-(h - atm.h0[b]) / atm.H[b]);
+      const double k = -0.5e3 * rho * bcInv * wn;
+      ax += k * wx;
+      ay += k * wy;
+      az += k * wz;
+    }
+  } else {
+    const float xf = (float)x, yf = (float)y, zf = (float)z;
+    const float rinvf = (float)rinv, rinv2f = (float)rinv2;
+    float bx = 0.f, by = 0.f, bz = 0.f;
+    if (mask & kPropJ3) {
+      const float k = (float)(-2.5 * kJ3 * kMuEarth * kREarth * kREarth * kREarth) *
+                      (rinv2f * rinv2f * rinv2f * rinvf);
+      const float z2 = zf * zf;
+      const float f = 3.0f * zf - 7.0f * z2 * zf * rinv2f;
+      const float z2r2 = z2 * rinv2f;
+      bx += k * xf * f;
+      by += k * yf * f;
+      // 6 z^2 - 7 z^4 / r^2 - 0.6 r^2 == z^2 (6 - 7 z^2/r^2) - 0.6 r^2
+      bz += k * (z2 * (6.0f - 7.0f * z2r2) - 0.6f * (float)r2);
+    }
+    if (mask & (kPropC22 | kPropS22)) {
+      const float C = (mask & kPropC22) ? (float)kC22 : 0.0f;
+      const float S = (mask & kPropS22) ? (float)kS22 : 0.0f;
+      const float c = e.cosTf, s = e.sinTf;
+      const float xe = c * xf + s * yf, ye = -s * xf + c * yf;
+      const float g = C * (xe * xe - ye * ye) + 2.0f * S * xe * ye;
+      const float k = (float)(3.0 * kMuEarth * kREarth * kREarth) * (rinv2f * rinv2f * rinvf);
+      const float axe = k * (2.0f * (C * xe + S * ye) - 5.0f * g * xe * rinv2f);
+      const float aye = k * (2.0f * (S * xe - C * ye) - 5.0f * g * ye * rinv2f);
+      bx += c * axe - s * aye;
+      by += s * axe + c * aye;
+      bz += k * (-5.0f * g * zf * rinv2f);
+    }
+#pragma unroll
+    for (int body = 0; body < 2; ++body) {
+      const uint32_t bit = body == 0 ? kPropSOL : kPropLUN;
+      if (!(mask & bit)) continue;
+      const float *sp = body == 0 ? e.sunf : e.moonf;
+      const float invS2 = body == 0 ? e.sunInvS2f : e.moonInvS2f;
+      const float mu = body == 0 ? (float)kMuSun : (float)kMuMoon;
+      // q = r.(r - 2s) / |s|^2 ;  a = -mu / |d|^3 (r + f(q) s),  d = s - r
+      const float q = (xf * (xf - 2.0f * sp[0]) + yf * (yf - 2.0f * sp[1]) + zf * (zf - 2.0f * sp[2])) * invS2;
+      const float dx = sp[0] - xf, dy = sp[1] - yf, dz = sp[2] - zf;
+      const float di = rsqrtf(dx * dx + dy * dy + dz * dz);
+      const float k = -mu * di * di * di;
+      const float f = battinF(q);
+      bx += k * (xf + f * sp[0]);
+      by += k * (yf + f * sp[1]);
+      bz += k * (zf + f * sp[2]);
+    }
+    if (mask & kPropSRP) {
+      const double proj = x * e.sunHat[0] + y * e.sunHat[1] + z * e.sunHat[2];
+      const bool shadow = proj < 0.0 && (r2 - proj * proj) < kREarth * kREarth;
+      if (!shadow) {
+        const float ux = xf - e.sunf[0], uy = yf - e.sunf[1], uz = zf - e.sunf[2];
+        const float ui = rsqrtf(ux * ux + uy * uy + uz * uz);
+        // (AU * ui)^2 * ui keeps every factor inside binary32 range
+        const float au = (float)kAU * ui;
+        const float k = (float)(kCR * kPSrp * 1.0e3) * (float)aom * (au * au * ui);
+        bx += k * ux;
+        by += k * uy;
+        bz += k * uz;
+      }
+    }
+    if (mask & kPropDRAG) {
+      const float wx = (float)v[0] + (float)kOmegaEarth * yf, wy = (float)v[1] - (float)kOmegaEarth * xf,
+                  wz = (float)v[2];
+      const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
+      const double h = rn - kREarth;
+      const int b = atmBand(atm, h);
+      const float rho = (float)atm.rho0[b] * expf(-(float)(h - atm.h0[b]) / (float)atm.H[b]);
+      const float k = -0.5e3f * rho * (float)bcInv * wn;
+      bx += k * wx;
+      by += k * wy;
+      bz += k * wz;
+    }
+    ax += (double)bx;
+    ay += (double)by;
+    az += (double)bz;
+  }
+  a[0] = ax;
+  a[1] = ay;
+  a[2] = az;
+}
+
+}  // namespace ladds

@@ -1,0 +1,118 @@
+// propagate.cuh -- Yoshida-4 propagation kernel (+ fused cell-key output).
+//
+// Replaces YoshidaIntegrator::integrate(false) (called at Simulation.cpp:297;
+// the integrator itself is in the non-vendored OrbitPropagator).  Form: DKD
+// composition of Yoshida (1990): drift c1, kick d1, drift c2, kick d2,
+// drift c2, kick d1, drift c1 -- three force evaluations per step at the
+// stage times t + c1 dt, t + (c1+c2) dt, t + (c1+2 c2) dt.
+//
+// One thread per object, state held in registers across `nSteps` steps, so
+// a multi-step launch touches HBM once (read 64 B + write 48 B per object).
+// Ephemeris entries of all stages of the launch live in __constant__ memory
+// (uniform across the warp).  The atmosphere table is staged in shared memory
+// (the band index diverges across the warp).
+#pragma once
+#include "forces.cuh"
+#include "state.cuh"
+
+namespace ladds {
+
+constexpr int kMaxEphSteps = 128;  // 3 * 128 entries * 160 B = 61 KB of constant memory
+__constant__ EphEntry c_eph[3 * kMaxEphSteps];
+__constant__ AtmRow c_atm[kAtmBands] = LADDS_ATM_TABLE;
+
+struct PropConsts {
+  double hc1, hc2, hd1, hd2;  // Yoshida coefficients * dt
+  uint32_t mask;
+};
+
+__device__ __forceinline__ uint32_t cellCoord(double v, double lo, double inv, int32_t n) {
+  // floor((v - lo) * inv) with exactly these two roundings; NaN -> 0; clamped
+  const double u = floor(__dmul_rn(__dsub_rn(v, lo), inv));
+  if (!(u >= 0.0)) return 0u;
+  if (u >= (double)n) return (uint32_t)(n - 1);
+  return (uint32_t)u;
+}
+
+__device__ __forceinline__ uint32_t cellKey(double x, double y, double z, const GridDesc &g) {
+  const uint32_t ix = cellCoord(x, g.boxMin[0], g.invCell, g.n[0]);
+  const uint32_t iy = cellCoord(y, g.boxMin[1], g.invCell, g.n[1]);
+  const uint32_t iz = cellCoord(z, g.boxMin[2], g.invCell, g.n[2]);
+  return (iz * (uint32_t)g.n[1] + iy) * (uint32_t)g.n[0] + ix;
+}
+
+template <bool SPLIT, bool KEYS>
+__global__ void __launch_bounds__(256) k_propagate(DevState s, int n, int nSteps, PropConsts pc, GridDesc g,
+                                                   uint32_t *__restrict__ keys, unsigned *__restrict__ status) {
+  __shared__ AtmShared atm;
+  for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
+    atm.h0[i] = c_atm[i].h0;
+    atm.rho0[i] = c_atm[i].rho0;
+    atm.H[i] = c_atm[i].H;
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t tag = s.tag[j];
+  double r[3] = {s.x[j], s.y[j], s.z[j]};
+  if (!tagDummy(tag)) {
+    double v[3] = {s.vx[j], s.vy[j], s.vz[j]};
+    const double aom = s.aom[j], bc = s.bc[j];
+    uint32_t mask = pc.mask;
+    if (tagAct(tag) == kEvasivePreserving) mask &= kPropKEP;  // Particle.h:48-52: Keplerian forces only
+    double a[3];
+    for (int st = 0; st < nSteps; ++st) {
+      const EphEntry *e = &c_eph[3 * st];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) r[k] += pc.hc1 * v[k];
+      accel<SPLIT>(mask, r, v, aom, bc, e[0], atm, a);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] += pc.hd1 * a[k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) r[k] += pc.hc2 * v[k];
+      accel<SPLIT>(mask, r, v, aom, bc, e[1], atm, a);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] += pc.hd2 * a[k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) r[k] += pc.hc2 * v[k];
+      accel<SPLIT>(mask, r, v, aom, bc, e[2], atm, a);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v[k] += pc.hd1 * a[k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) r[k] += pc.hc1 * v[k];
+    }
+    if (!(isfinite(r[0]) && isfinite(r[1]) && isfinite(r[2]) && isfinite(v[0]) && isfinite(v[1]) &&
+          isfinite(v[2])))
+      atomicOr(status, 1u);
+    s.x[j] = r[0];
+    s.y[j] = r[1];
+    s.z[j] = r[2];
+    s.vx[j] = v[0];
+    s.vy[j] = v[1];
+    s.vz[j] = v[2];
+  }
+  if (KEYS) keys[j] = cellKey(r[0], r[1], r[2], g);
+}
+
+// Ephemeris of the stage times of `nSteps` steps starting at iteration `iter`
+// (one thread per stage), written to a global staging table that the host then
+// copies into c_eph.
+__global__ void k_ephemeris(EphEntry *__restrict__ out, int nSteps, int64_t iter, double t0, double dt, double hc1,
+                            double hc2, double jdEpoch, double theta0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nSteps) return;
+  const int st = i / 3, stage = i % 3;
+  const double tn = t0 + (double)(iter + st) * dt;
+  double tau = tn + hc1;
+  if (stage >= 1) tau += hc2;
+  if (stage >= 2) tau += hc2;
+  ephemeris(jdEpoch, theta0, tau, out[i]);
+}
+
+__global__ void k_cell_keys(const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
+                            int n, GridDesc g, uint32_t *__restrict__ keys) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) keys[j] = cellKey(x[j], y[j], z[j], g);
+}
+
+}  // namespace ladds

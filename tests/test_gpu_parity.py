@@ -1,0 +1,294 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the CPU oracle.
+
+Bar: conjunction records and cell-sort order bit-exact; positions within
+1e-6 km after 100 FP64 steps (Kepler + J2 and the full set); split precision
+within 1e-6 km of the FP64 oracle after 100 steps as well.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from helpers import describe_diff, from_lists, records_equal, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def capi():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from ladds_b200 import build, capi
+
+    build.build_gpu()
+    return capi
+
+
+def ctx_for(capi, **kw):
+    return capi.Context(capi.default_config(**kw))
+
+
+# ---------------------------------------------------------------- known answers
+def _collisions(recs, capi):
+    return recs[(recs["flags"] & capi.PAIR_COLLISION) != 0]
+
+
+def test_three_particles_gpu(capi, oracle):
+    pop = from_lists([[i / 1000.0, 0, 0] for i in range(3)], [[0, float(i), 0] for i in range(3)], [0, 1, 2],
+                     [0, 0, 0], [1.0] * 3, [0.6] * 3)
+    with ctx_for(capi, cutoff=1.0, minDetectionRadius=0.01, evasionCutoff=0.1) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(10.0)
+    col = _collisions(recs, capi)
+    got = sorted((int(r["idA"]), int(r["idB"]), float(r["dl2"]), tuple(r["point"])) for r in col)
+    assert got == [(0, 1, 1e-6, (0.0005, 0.0, 0.0)), (1, 2, 1e-6, (0.0015, 0.0, 0.0))]
+    p = oracle.scan_params(cutoff=1.0, dt=10.0, min_detection_radius=0.01, evasion_cutoff=0.1)
+    assert records_equal(recs, oracle.scan_bruteforce(to_oracle(oracle, pop), p))
+
+
+def test_mix_activity_states_gpu(capi, oracle):
+    rs = [[0, 0, 0], [0, 0, 0.1], [0.1, 0, 0], [0.1, 0, 0.1], [0, 0.1, 0], [0, 0.1, 0.1], [0.1, 0.1, 0],
+          [0.1, 0.1, 0.1]]
+    ids = [0, 0, 1, 1, 2, 3, 4, 5]
+    acts = [0, 0, 0, 0, 1, 1, 2, 2]
+    radii = [0.001, 0.001, 1, 1, 1, 1, 1, 1]
+    pop = from_lists(rs, [[0, 0, 0]] * 8, ids, acts, [1.0] * 8, radii)
+    with ctx_for(capi, cutoff=1.0, minDetectionRadius=0.01, evasionCutoff=0.1) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(10.0)
+    col = _collisions(recs, capi)
+    assert len(col) == 14
+    assert np.all(np.isnan(col["dl2"]))  # the reference's 0/0 path
+    p = oracle.scan_params(cutoff=1.0, dt=10.0, min_detection_radius=0.01, evasion_cutoff=0.1)
+    assert records_equal(recs, oracle.scan_bruteforce(to_oracle(oracle, pop), p))
+
+
+@pytest.mark.parametrize("factor,expected", [(1.0, 0), (2.0, 1)])
+def test_collision_distance_factor_gpu(capi, factor, expected):
+    pop = from_lists([[0, 0, 0], [3e-3, 0, 0]], [[1, 0, 0], [-1, 0, 0]], [1, 2], [0, 0], [1.0, 1.0], [1.0, 1.0])
+    with ctx_for(capi, cutoff=80.0, collisionDistanceFactor=factor, minDetectionRadius=0.1) as ctx:
+        ctx.upload(pop)
+        assert len(_collisions(ctx.conjunctions(1.0), capi)) == expected
+
+
+@pytest.mark.parametrize("case", json.load(open(os.path.join(GOLDEN, "interpolation_cases.json")))["cases"])
+def test_linear_interpolation_gpu(capi, case):
+    pop = from_lists([case["x1"], case["x2"]], [case["v1"], case["v2"]], [0, 1], [0, 0], [1.0, 1.0], [1000.0] * 2)
+    with ctx_for(capi, cutoff=80.0, collisionDistanceFactor=10.0, minDetectionRadius=0.1) as ctx:
+        ctx.upload(pop)
+        col = _collisions(ctx.conjunctions(case["dt"]), capi)
+    assert len(col) == 1
+    assert float(col[0]["dl2"]) == case["expected_dl2"]
+    assert tuple(float(v) for v in col[0]["point"]) == tuple(case["expected_point"])
+
+
+# ------------------------------------------------------- dense random populations
+def dense_population(seed, n=6000, span=250.0):
+    """Objects in a box around (7000, 0, 0) km: many cutoff candidates and
+    records in every list; includes duplicated states (NaN path), shared
+    parents, duplicated ids, every activity state and deleted objects."""
+    rng = np.random.default_rng(seed)
+    r = np.array([7000.0, 0.0, 0.0]) + rng.uniform(-span / 2, span / 2, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    v = d * rng.uniform(0.0, 8.0, size=(n, 1))
+    r[n - 10:] = r[:10]  # identical states
+    v[n - 10:] = v[:10]
+    radius = np.exp(rng.uniform(np.log(0.01), np.log(5.0), n))
+    mass = 2700 * 4 / 3 * np.pi * radius ** 3
+    ids = np.arange(n, dtype=np.uint64)
+    ids[100:110] = ids[0:10]  # duplicate ids
+    parent = np.full(n, np.uint64(0xFFFFFFFFFFFFFFFF))
+    parent[200:260] = np.uint64(777)
+    act = rng.choice([0, 0, 0, 1, 2], size=n).astype(np.int8)
+    return dict(x=r[:, 0], y=r[:, 1], z=r[:, 2], vx=v[:, 0], vy=v[:, 1], vz=v[:, 2], radius=radius,
+                aom=np.pi * radius ** 2 * 1e-6 / mass, bc_inv=2.2 * np.pi * radius ** 2 / mass, id=ids,
+                parent=parent, activity=act)
+
+
+DENSE_BOX = ([6500.0, -500.0, -500.0], [7500.0, 500.0, 500.0])
+DENSE_KW = dict(cutoff=20.0, collisionDistanceFactor=2000.0, minDetectionRadius=0.05, evasionCutoff=3.0,
+                conjunctionThreshold=2.0, boxMin=DENSE_BOX[0], boxMax=DENSE_BOX[1])
+
+
+@pytest.mark.parametrize("cell", [0.0, 7.0, 10.0, 33.0, 60.0])
+def test_scan_bitexact_vs_oracle(capi, oracle, cell):
+    pop = dense_population(11)
+    dt = 10.0
+    with ctx_for(capi, cellSize=cell, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(dt)
+        keys, slots = ctx.cell_order()
+        dims, reach, cs = ctx.grid()
+    p = oracle.scan_params(cutoff=20.0, dt=dt, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    grid = oracle.make_grid(DENSE_BOX[0], DENSE_BOX[1], cell, 20.0)
+    assert tuple(grid.n) == dims and grid.reach == reach and grid.cellSize == cs
+    opop = to_oracle(oracle, pop)
+    ref = oracle.scan_cells(opop, p, grid)
+    brute = oracle.scan_bruteforce(opop, p)
+    assert records_equal(ref, brute), describe_diff(ref, brute)
+    assert len(recs) > 100
+    for flag in (capi.PAIR_COLLISION, capi.PAIR_EVASION, capi.PAIR_CONJUNCTION):
+        assert np.any(recs["flags"] & flag)
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+    okeys = oracle.cell_keys(opop, grid)
+    operm = oracle.stable_sort(okeys)
+    assert np.array_equal(slots, operm)
+    assert np.array_equal(keys, okeys[operm])
+
+
+def test_scan_with_deleted_objects(capi, oracle):
+    pop = dense_population(12, n=3000)
+    dead = np.arange(0, 3000, 7, dtype=np.uint32)
+    with ctx_for(capi, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        ctx.mark_deleted(dead)
+        recs = ctx.conjunctions(10.0)
+    opop = to_oracle(oracle, pop)
+    opop.dummy[dead] = 1
+    p = oracle.scan_params(cutoff=20.0, dt=10.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    ref = oracle.scan_bruteforce(opop, p)
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+    assert not np.isin(recs["slotA"], dead).any() and not np.isin(recs["slotB"], dead).any()
+
+
+def test_pair_buffer_overflow_retries(capi, oracle):
+    pop = dense_population(13, n=4000)
+    with ctx_for(capi, pairCapacity=1, **DENSE_KW) as small, ctx_for(capi, **DENSE_KW) as big:
+        small.upload(pop)
+        big.upload(pop)
+        a = small.step(3, cap=1 << 20)  # device buffer of one record: overflow, grow, re-run
+        b = big.step(3)
+        c = small.step(2, cap=1)  # caller buffer too small: rolled back, re-called with the needed size
+        d = big.step(2)
+    assert a.stats.retries >= 1
+    assert records_equal(a.records, b.records)
+    assert records_equal(c.records, d.records)
+
+
+# --------------------------------------------------------------- propagation
+def _state(pop):
+    return np.stack([pop["x"], pop["y"], pop["z"]], 1), np.stack([pop["vx"], pop["vy"], pop["vz"]], 1)
+
+
+def test_two_body_fixture_gpu(capi):
+    d = json.load(open(os.path.join(GOLDEN, "two_body_10s.json")))
+    r0, v0, r1, v1 = (np.asarray(d[k]) for k in ("r0", "v0", "r1", "v1"))
+    pop = dict(x=r0[:, 0], y=r0[:, 1], z=r0[:, 2], vx=v0[:, 0], vy=v0[:, 1], vz=v0[:, 2], radius=np.ones(10),
+               aom=np.zeros(10), bc_inv=np.zeros(10), id=np.arange(10))
+    for dt, steps in ((10.0, 1), (1.0, 10)):
+        with ctx_for(capi, deltaT=dt, componentMask=capi.KEP) as ctx:
+            ctx.upload(pop)
+            ctx.integrate(steps)
+            r, v = _state(ctx.download())
+        assert np.max(np.abs(r - r1)) < 2e-6 and np.max(np.abs(v - v1)) < 2e-9
+
+
+@pytest.mark.parametrize("mask_name,precision", [("KEPJ2", 0), ("FULL", 0), ("FULL", 1), ("KEPJ2", 1)])
+def test_propagation_vs_oracle_100_steps(capi, oracle, mask_name, precision):
+    mask = capi.KEP | capi.J2 if mask_name == "KEPJ2" else capi.PROP_ALL
+    pop = capi.generate_population(0, 1000, 10000)
+    pop["activity"][::50] = capi.EVASIVE_PRESERVING
+    with ctx_for(capi, componentMask=mask, precision=precision) as ctx:
+        ctx.upload(pop)
+        ctx.integrate(100)
+        got = ctx.download()
+    opop = to_oracle(oracle, pop)
+    oracle.propagate(opop, mask, 10.0, 100)
+    rg, vg = _state(got)
+    ro = np.stack([opop.x, opop.y, opop.z], 1)
+    vo = np.stack([opop.vx, opop.vy, opop.vz], 1)
+    assert np.max(np.abs(rg - ro)) < 1e-6, np.max(np.abs(rg - ro))
+    assert np.max(np.abs(vg - vo)) < 1e-9
+    assert np.array_equal(got["id"], pop["id"])
+
+
+def test_graph_replay_equals_eager(capi):
+    pop = dense_population(14, n=5000)
+    outs = []
+    for graphs in (0, 1):
+        with ctx_for(capi, useGraphs=graphs, deltaT=1.0, componentMask=capi.KEP | capi.J2, **DENSE_KW) as ctx:
+            ctx.upload(pop)
+            r1 = ctx.step(7)
+            r2 = ctx.step(7)  # second call replays the cached graph
+            outs.append((r1.records, r2.records, ctx.download(), ctx.cell_order()))
+    a, b = outs
+    assert records_equal(a[0], b[0]) and records_equal(a[1], b[1])
+    for k in ("x", "vz", "id"):
+        assert np.array_equal(a[2][k], b[2][k])
+    assert np.array_equal(a[3][0], b[3][0]) and np.array_equal(a[3][1], b[3][1])
+
+
+def test_step_records_match_oracle_scan_of_gpu_state(capi, oracle):
+    """Each iteration's records equal the oracle's scan of the state the GPU
+    produced for that iteration (bit-exact)."""
+    pop = dense_population(15, n=4000)
+    p = oracle.scan_params(cutoff=20.0, dt=1.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    with ctx_for(capi, deltaT=1.0, componentMask=capi.KEP | capi.J2, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        for it in range(3):
+            res = ctx.step(1)
+            state = ctx.download()
+            ref = oracle.scan_bruteforce(to_oracle(oracle, state), p, step=it)
+            assert records_equal(res.records, ref), describe_diff(res.records, ref)
+
+
+def test_timesteps_per_collision_detection(capi):
+    """SimulationTest.cpp:144-193: two bodies approaching at 20 km/s, k = 2;
+    conjunction counts 0 / 0 / 1 after 1 / 2 / 3 iterations."""
+    rmin = 6378.137 + 150.0
+    pop = from_lists([[rmin + 100.0, 20.0, 0.0], [rmin + 100.0, -20.0, 0.0]], [[0, -10.0, 0], [0, 10.0, 0]], [0, 1],
+                     [0, 0], [1.0, 1.0], [1.0, 1.0])
+    for iterations, expected in ((1, 0), (2, 0), (3, 1)):
+        with ctx_for(capi, deltaT=1.0, componentMask=capi.KEP, timestepsPerCollisionDetection=2) as ctx:
+            ctx.upload(pop)
+            res = ctx.step(iterations)
+            assert int(res.stats.collisions) == expected, iterations
+
+
+def test_nonfinite_state_is_reported_and_rolled_back(capi):
+    pop = capi.generate_population(0, 5, 1000)
+    pop["x"][3] = pop["y"][3] = pop["z"][3] = 0.0  # at the geocentre: 1/r -> inf
+    with ctx_for(capi) as ctx:
+        ctx.upload(pop)
+        with pytest.raises(capi.LaddsError) as e:
+            ctx.step(2)
+        assert e.value.code == capi.ERR_NONFINITE
+        back = ctx.download()
+        assert np.array_equal(back["x"], pop["x"]) and ctx.iteration() == 0
+
+
+def test_burnup_removal_and_append(capi):
+    pop = capi.generate_population(0, 6, 5000)
+    low = capi.generate_population(0, 99, 100)
+    scale = (6378.137 + 100.0) / np.linalg.norm(np.stack([low["x"], low["y"], low["z"]], 1), axis=1)
+    for k in ("x", "y", "z"):
+        low[k] = low[k] * scale
+    low["id"] = np.arange(10000, 10100, dtype=np.uint64)
+    with ctx_for(capi) as ctx:
+        ctx.upload(pop)
+        ctx.conjunctions(10.0)  # reorder the device arrays first
+        ctx.append(low)
+        assert ctx.size() == 5100
+        removed = ctx.remove_below(150.0)
+        assert sorted(removed.tolist()) == list(range(10000, 10100))
+        back = ctx.download()
+    assert np.array_equal(back["id"], pop["id"]) and np.array_equal(back["x"], pop["x"])
+
+
+def test_clear_parents(capi):
+    pop = capi.generate_population(0, 8, 1000)
+    pop["parent"][:] = 5
+    with ctx_for(capi) as ctx:
+        ctx.upload(pop)
+        ctx.clear_parents()
+        assert np.all(ctx.download()["parent"] == capi.SIZE_MAX)
