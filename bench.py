@@ -1,0 +1,460 @@
+"""Benchmark of the LADDS propagate + conjunction hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): 1,000,000
+objects from the seeded population 0 (a = R + U[400,1500] km, e U[0,0.02],
+i U[0,180] deg, radius logU[0.01,5] m), full perturbation set (KEP, J2, J3,
+C22, S22, Sun, Moon, SRP, drag), dt = 10 s, conjunction scan every step with
+the 80 km cell-list cutoff and the 0.1 km conjunction threshold.
+
+One step = one iteration of the reference loop (Simulation.cpp:287-415):
+Yoshida-4 step of every object, then the conjunction scan.  ``value`` is the
+split-precision object-steps/s with the population resident in HBM; the FP64
+figure, their ratio and the one-day RMS drift of split vs FP64 are reported
+beside it.  ``e2e`` runs the same steps through the C ABI in the host-owned
+mode of the drop-in: per step the positions/velocities go host->device from
+pinned memory, the step runs, positions/velocities and the conjunction
+records come back.  ``--impl reference`` times the CPU restatement of the
+reference path (the oracle; the reference itself cannot be built here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_OBJECTS = 1_000_000
+SEED = 1001
+METRIC = "object-steps/s, mixed vs FP64 on B200 at <=1 m/day drift; adjoint/forward time"
+WORKLOAD = "population 0, 1e6 objects, full perturbations, dt 10 s, scan every step (80 km cutoff, 0.1 km threshold)"
+STEPS_PER_DAY = 8640
+
+
+# ----------------------------------------------------------------- helpers
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        import datetime
+
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ----------------------------------------------------------- algorithmic work
+def algorithmic_units(n):
+    """Per-step algorithmic bytes and flops of each phase (definitions in DESIGN.md)."""
+    passes = 3
+    return {
+        # read r, v, aom, bcInv, tag (68 B), write r, v (48 B), write the cell key (4 B)
+        "propagate": {"bytes": n * 120, "flops_fp64": None},
+        # 3 radix passes: read key (+value) for the histogram and the scatter, write key+value
+        "sort": {"bytes": n * (4 + passes * (4 + 8 + 8))},
+        # gather 92 B/object into cell order, write 92 B + 32 B packed positions, read perm
+        "cell": {"bytes": n * (92 + 92 + 32 + 4 + 4)},
+        # read own object (92 B) once; neighbours come from L2
+        "scan": {"bytes": n * 92},
+    }
+
+
+def propagation_flops(mask_full=True):
+    # counted FP operations per force evaluation of the restated model
+    f_eval = 208 if mask_full else 33
+    return 3 * f_eval + 42
+
+
+def measure_peaks():
+    try:
+        import ctypes as C
+
+        from ladds_b200 import build
+
+        lib = C.CDLL(build.build_peaks())
+        f64, f32 = C.c_double(), C.c_double()
+        lib.ladds_measure_fma_tflops.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        if lib.ladds_measure_fma_tflops(0, C.byref(f64), C.byref(f32)) == 0:
+            return f64.value, f32.value
+    except Exception:
+        pass
+    return None, None
+
+
+def measured_peaks_file():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_baseline(n_objects, seed, budget_s=20.0, steps_cap=None):
+    """Times the oracle (C + OpenMP restatement of the reference path) on the host
+    cores: full Yoshida step of the full force set + linked-cell scan."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+
+    from ladds_b200 import capi
+
+    pop = capi.generate_population(0, seed, n_objects)
+    opop = O.Population(pop["x"], pop["y"], pop["z"], pop["vx"], pop["vy"], pop["vz"], pop["radius"], pop["aom"],
+                        pop["bc_inv"], pop["id"], pop["parent"], pop["activity"])
+    grid = O.make_grid([-10000.0] * 3, [10000.0] * 3, 0.0, 80.0)
+    params = O.scan_params(cutoff=80.0, dt=10.0)
+    cores = os.cpu_count() or 1
+    # one full step first, to size the sample
+    t0 = time.perf_counter()
+    O.propagate(opop, O.FULL, 10.0, 1, t0=0.0)
+    O.scan_cells(opop, params, grid, step=0)
+    t_full = time.perf_counter() - t0
+    return O, opop, grid, params, t_full, cores
+
+
+def wedge_population(pop, frac):
+    """Objects with longitude in [0, 2 pi frac): a same-density sample."""
+    lon = np.arctan2(pop["y"], pop["x"]) % (2 * math.pi)
+    keep = lon < 2 * math.pi * frac
+    return {k: (v[keep] if isinstance(v, np.ndarray) else v) for k, v in pop.items()}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement on all host cores, bounded sample per step."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+
+    from ladds_b200 import capi
+
+    pop = capi.generate_population(0, SEED, args.n_objects)
+    grid = O.make_grid([-10000.0] * 3, [10000.0] * 3, 0.0, 80.0)
+    params = O.scan_params(cutoff=80.0, dt=10.0)
+
+    def to_o(p):
+        return O.Population(p["x"], p["y"], p["z"], p["vx"], p["vy"], p["vz"], p["radius"], p["aom"], p["bc_inv"],
+                            p["id"], p["parent"], p["activity"])
+
+    # size the per-step sample so that warm-up + timed steps fit the budget
+    probe = to_o(wedge_population(pop, 0.05))
+    t0 = time.perf_counter()
+    O.propagate(probe, O.FULL, 10.0, 1)
+    O.scan_cells(probe, params, grid)
+    t_probe = max(time.perf_counter() - t0, 1e-4)
+    per_obj = t_probe / max(probe.n, 1)
+    budget = args.reference_budget
+    m_target = budget / max(args.steps + args.warmup, 1) / per_obj
+    frac = min(1.0, max(m_target / args.n_objects, 1e-4))
+    sample = to_o(wedge_population(pop, frac))
+    for w in range(args.warmup):
+        O.propagate(sample, O.FULL, 10.0, 1, t0=10.0 * w)
+        O.scan_cells(sample, params, grid, step=w)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        O.propagate(sample, O.FULL, 10.0, 1, t0=10.0 * (args.warmup + s))
+        O.scan_cells(sample, params, grid, step=args.warmup + s)
+    el = time.perf_counter() - t0
+    value = sample.n * args.steps / el
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_objects": args.n_objects, "sample_objects": sample.n,
+                   "sample": f"longitude wedge of {frac:.4f} of the population (same density)",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "object-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample.n} objects (longitude wedge, same density) x {args.steps} steps"},
+        "e2e": {"value": value, "unit": "object-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=STEPS_PER_DAY)
+    ap.add_argument("--warmup", type=int, default=16)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-objects", type=int, default=N_OBJECTS)
+    ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--no-drift", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--reference-budget", type=float, default=150.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    from ladds_b200 import build, capi
+
+    build.build_gpu()
+    n = args.n_objects
+    pop = capi.generate_population(0, SEED + rank, n)  # replicas: one population per rank
+
+    def make_ctx(precision, graphs=1):
+        return capi.Context(capi.default_config(componentMask=capi.PROP_ALL, precision=precision, device=local,
+                                                useGraphs=graphs, pairCapacity=1 << 16))
+
+    results = {}
+    for name, prec in (("split", capi.PRECISION_SPLIT), ("fp64", capi.PRECISION_FP64)):
+        ctx = make_ctx(prec)
+        ctx.upload(pop)
+        ctx.step(args.warmup)
+        # the timed call captures its CUDA graphs (one per 128-step chunk) before
+        # its first timing event, so device time covers the replay only
+        dist_barrier(world)
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            res = ctx.step(args.steps)
+            wall = time.perf_counter() - t0
+        dev_ms = dist_max(res.stats.deviceMs, world)
+        results[name] = dict(ms=dev_ms, wall=wall, records=int(res.stats.records), clocks=clk.summary(),
+                             conj=int(res.stats.conjunctions), coll=int(res.stats.collisions))
+        # per-phase device times (eager, CUDA events on the library stream), same workload
+        ctx.set_profiling(True)
+        ctx.step(min(args.steps, 64))
+        pt = ctx.phase_times()
+        results[name]["phases"] = {"propagate": pt.propagateMs, "sort": pt.sortMs, "cell": pt.cellMs,
+                                   "scan": pt.scanMs, "steps": min(args.steps, 64),
+                                   "launches": {"propagate": pt.propagateLaunches, "sort": pt.sortLaunches,
+                                                "cell": pt.cellLaunches, "scan": pt.scanLaunches}}
+        ctx.set_profiling(False)
+        ctx.close()
+
+    # one-day drift of split vs FP64 (both from the same start state)
+    drift = None
+    if not args.no_drift and rank == 0:
+        finals = {}
+        for name, prec in (("split", capi.PRECISION_SPLIT), ("fp64", capi.PRECISION_FP64)):
+            ctx = make_ctx(prec)
+            ctx.upload(pop)
+            r = ctx.step(STEPS_PER_DAY)
+            d = ctx.download()
+            finals[name] = (np.stack([d["x"], d["y"], d["z"]], 1), r.records)
+            ctx.close()
+        dr = finals["split"][0] - finals["fp64"][0]
+        rms_m = float(np.sqrt(np.mean(np.sum(dr * dr, 1)))) * 1e3
+        key = lambda recs: set(zip(recs["step"].tolist(), recs["idA"].tolist(), recs["idB"].tolist(),
+                                   (recs["flags"] & 7).tolist()))
+        a, b = key(finals["split"][1]), key(finals["fp64"][1])
+        drift = {"rms_m_one_day": rms_m, "max_m_one_day": float(np.max(np.linalg.norm(dr, axis=1)) * 1e3),
+                 "records_split": len(a), "records_fp64": len(b), "records_only_in_one": len(a ^ b)}
+
+    # end to end through the C ABI, host-owned container: H2D state, step, D2H state + records
+    e2e = None
+    try:
+        import torch
+
+        ctx = make_ctx(capi.PRECISION_SPLIT, graphs=0)
+        ctx.upload(pop)
+        ctx.step(2)
+        pinned = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(6)]
+        st = ctx.get_state()
+        for a, b in zip(pinned, st):
+            a[:] = b
+        out = np.zeros(1 << 16, dtype=capi.PAIR_DTYPE)
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        rec_bytes = 0
+        for _ in range(args.e2e_steps):
+            ctx.set_state(*pinned)
+            r = ctx.step(1, out=out)
+            rec_bytes += len(r.records) * 64 + 8
+            ctx._check(ctx._L.ladds_gpu_get_state(ctx.handle, n, *[a.ctypes.data_as(capi.C.c_void_p)
+                                                                    for a in pinned]))
+        el = dist_max(time.perf_counter() - t0, world)
+        e2e = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
+               "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": int(48 * n + rec_bytes / args.e2e_steps),
+               "steps": args.e2e_steps, "mode": "host-owned state (set_state / step(1) / get_state, pinned)"}
+        ctx.close()
+    except Exception as ex:  # noqa: BLE001
+        e2e = {"value": None, "unit": "object-steps/s", "error": str(ex)[:200]}
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    split, fp64 = results["split"], results["fp64"]
+    value = world * n * args.steps / (split["ms"] * 1e-3)
+    fp64_value = world * n * args.steps / (fp64["ms"] * 1e-3)
+
+    # roofline of the dominant kernel (from the per-phase device times)
+    units = algorithmic_units(n)
+    ph = split["phases"]
+    per = {k: ph[k] / ph["steps"] for k in ("propagate", "sort", "cell", "scan")}
+    dominant = max(per, key=per.get)
+    peaks = measured_peaks_file()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    f64_peak, f32_peak = measure_peaks()
+    kernels = {}
+    for k, ms in per.items():
+        gbs = units[k]["bytes"] / (ms * 1e-3) / 1e9 if ms > 0 else None
+        kernels[k] = {"ms_per_step": ms, "algorithmic_bytes": units[k]["bytes"], "achieved_gbs": gbs,
+                      "hbm_frac": gbs / hbm_peak if gbs else None}
+    fp64_ph = fp64["phases"]
+    prop64_ms = fp64_ph["propagate"] / fp64_ph["steps"]
+    prop_flops = propagation_flops() * n
+    kernels["propagate_fp64_mode"] = {"ms_per_step": prop64_ms, "algorithmic_flops": prop_flops,
+                                      "achieved_tflops": prop_flops / (prop64_ms * 1e-3) / 1e12,
+                                      "fp64_fma_peak_tflops_measured": f64_peak}
+    if f64_peak:
+        kernels["propagate_fp64_mode"]["fp64_frac"] = kernels["propagate_fp64_mode"]["achieved_tflops"] / f64_peak
+    dk = kernels[dominant]
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["achieved_gbs"], "peak": hbm_peak,
+                "unit": "GB/s", "frac": dk["hbm_frac"], "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+
+    cpu = None
+    if not args.no_cpu and world == 1:
+        try:
+            O, opop, grid, params, t_full, cores = cpu_baseline(n, SEED)
+            steps = max(1, int(args.cpu_budget / max(t_full, 1e-3)))
+            t0 = time.perf_counter()
+            for s in range(steps):
+                O.propagate(opop, O.FULL, 10.0, 1, t0=10.0 * (s + 1))
+                O.scan_cells(opop, params, grid, step=s + 1)
+            el = time.perf_counter() - t0
+            cpu = {"value": n * steps / el, "unit": "object-steps/s", "cores": cores, "kind": "port",
+                   "sample": f"{steps} full steps of the 1e6-object workload (oracle, OpenMP {cores} threads)"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "error": str(ex)[:200]}
+
+    launches_per_step = sum(split["phases"]["launches"].values()) / split["phases"]["steps"] + 1  # + k_advance
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "object-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": split["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64+f32 (split)",
+        "data": "synthetic (seeded population 0)",
+        "config": {"workload": WORKLOAD, "n_objects": n, "precision": "split", "dt_s": 10.0,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2: per-step working set ~450 MB (state 2 x 92 MB + keys + packed)"},
+        "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
+        "mixed_over_fp64": value / fp64_value,
+        "drift": drift,
+        "adjoint_over_forward": None,
+        "records": {"split": split["records"], "fp64": fp64["records"]},
+        "e2e": e2e,
+        "roofline": roofline,
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "clocks": split["clocks"],
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "wall_s": {"split": split["wall"], "fp64": fp64["wall"]},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -107,7 +107,7 @@ typedef struct {
   double boxMin[3], boxMax[3];    /* cell-grid box [km]; objects outside are clamped   */
   int32_t device;                 /* CUDA device ordinal                               */
   int32_t propagateBlock;         /* threads per block of the propagation kernel (0: 256) */
-  int32_t scanBlock;              /* threads per block of the pair scan (0: 128)       */
+  int32_t scanBlock;              /* threads per block of the candidate evaluation (0: 256) */
   int32_t useGraphs;              /* capture multi-iteration calls in CUDA graphs      */
   uint64_t pairCapacity;          /* initial device pair-buffer capacity (0: auto)     */
 } ladds_gpu_config;

@@ -68,6 +68,23 @@ def build_gpu(force: bool = False, verbose: bool = False, ptxas_info: bool = Fal
     return GPU_LIB
 
 
+PEAKS_LIB = os.path.join(PKG, "libladds_peaks.so")
+
+
+def build_peaks(force: bool = False, verbose: bool = False) -> str:
+    """FMA-pipe throughput diagnostic used by bench.py for the roofline denominators."""
+    src = os.path.join(CSRC, "peaks.cu")
+    if not force and _newer(PEAKS_LIB, [src]):
+        return PEAKS_LIB
+    cmd = [nvcc(), *NVCC_ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o", PEAKS_LIB, src]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    return PEAKS_LIB
+
+
 def build_host(force: bool = False, verbose: bool = False) -> str:
     srcs = _sources(os.path.join(HOST_DIR, "src"), (".cpp",))
     if not srcs:
@@ -89,6 +106,7 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
 
 def build(force: bool = False, verbose: bool = False) -> None:
     build_gpu(force=force, verbose=verbose)
+    build_peaks(force=force, verbose=verbose)
     build_host(force=force, verbose=verbose)
 
 

@@ -1,0 +1,248 @@
+// cell_sort.cuh -- cell order of the population: integer bucket sort on the
+// cell keys, most significant "digit" first.
+//
+// Replaces the cell binning of the AutoPas LinkedCells container (external,
+// configured at Simulation.cpp:59-120).  The order produced is the sort by
+// (cell key, slot): identical to a stable sort by key of the population in
+// slot order, and independent of the order the arrays are in before the call.
+//
+//   1. k_bucket_count: objects per cell row (row = key / nx; warp-aggregated
+//      atomics), then an exclusive scan of the counts = the row-start table
+//      that the pair scan uses.
+//   2. k_bucket_scatter: each object to its row bucket (warp-aggregated cursor
+//      atomics), with its sort record (ix << 32 | slot) and source index.
+//   3. k_bucket_sort_small: one warp per row of <= 32 objects, bitonic sort of
+//      the records in registers; longer rows are listed for
+//   4. k_bucket_sort_large: one CTA per listed row, bitonic sort in shared
+//      memory (<= kLargeRow objects) or in global memory beyond that.
+// The bitonic network is the variant whose comparators all put the minimum at
+// the lower index, so a row of any length is sorted as if padded with +inf
+// without touching the padding.  No kernel waits on another CTA.
+#pragma once
+#include <cstdint>
+
+#include "state.cuh"
+
+namespace ladds {
+
+constexpr int kLargeRow = 4096;  // objects sorted in shared memory by one CTA (48 KB)
+constexpr int kBucketThreads = 256;
+
+__device__ __forceinline__ uint32_t laneMaskLt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const uint32_t *__restrict__ keys, int n,
+                                                                 uint32_t nx, uint32_t *__restrict__ rowCount) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = j < n;
+  const uint32_t row = valid ? keys[j] / nx : 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, row);
+  if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&rowCount[row], (uint32_t)__popc(peers));
+}
+
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const uint32_t *__restrict__ keys,
+                                                                   const uint32_t *__restrict__ tags, int n,
+                                                                   uint32_t nx, const uint32_t *__restrict__ rowStart,
+                                                                   uint32_t *__restrict__ rowCursor,
+                                                                   unsigned long long *__restrict__ rec,
+                                                                   uint32_t *__restrict__ src) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool valid = j < n;
+  const uint32_t key = valid ? keys[j] : 0u;
+  const uint32_t row = valid ? key / nx : 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, row);
+  const int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (valid && lane == leader) base = atomicAdd(&rowCursor[row], (uint32_t)__popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!valid) return;
+  const uint32_t pos = rowStart[row] + base + (uint32_t)__popc(peers & laneMaskLt());
+  if (pos >= (uint32_t)n) return;  // only reachable with inconsistent counts
+  const uint32_t ix = key - row * nx;
+  rec[pos] = ((unsigned long long)ix << 32) | tagSlot(tags[j]);
+  src[pos] = (uint32_t)j;
+}
+
+// comparator i of stage (k, jj) of the all-ascending bitonic network
+__device__ __forceinline__ void bitonicPair(uint32_t i, uint32_t k, uint32_t jj, uint32_t &lo, uint32_t &hi) {
+  if (jj == k / 2) {  // flip stage
+    const uint32_t g = i / jj, w = i % jj;
+    lo = g * k + w;
+    hi = g * k + k - 1 - w;
+  } else {
+    const uint32_t g = i / jj, w = i % jj;
+    lo = g * 2 * jj + w;
+    hi = lo + jj;
+  }
+}
+
+// Warp bitonic sort of 32*S records held S per lane, element e = slot*32 + lane.
+// Comparator partners at distance < 32 are other lanes (shuffles), at distance
+// >= 32 other slots of the same lane; the flip stages pair e with e ^ (k-1).
+template <int S>
+__device__ __forceinline__ void warpBitonic(unsigned long long (&v)[S], uint32_t (&p)[S], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * S; k <<= 1) {
+#pragma unroll
+    for (int jj = k / 2; jj > 0; jj >>= 1) {
+      const bool flip = jj == k / 2;
+      const int mask = flip ? k - 1 : jj;
+      if (mask < 32) {  // partner in another lane, same slot
+        const int pl = lane ^ mask;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const unsigned long long ov = __shfl_sync(0xffffffffu, v[s], pl);
+          const uint32_t op = __shfl_sync(0xffffffffu, p[s], pl);
+          const bool lower = lane < pl;
+          if (lower ? (ov < v[s]) : (ov > v[s])) {
+            v[s] = ov;
+            p[s] = op;
+          }
+        }
+      } else if (!flip) {  // partner in the same lane: slot ^ (jj / 32)
+        const int sm = jj / 32;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const int t = s ^ sm;
+          if (t > s && v[t] < v[s]) {
+            const unsigned long long tv = v[s];
+            v[s] = v[t];
+            v[t] = tv;
+            const uint32_t tp = p[s];
+            p[s] = p[t];
+            p[t] = tp;
+          }
+        }
+      } else {  // flip across lanes and slots: lane ^ 31, slot ^ (k/32 - 1)
+        const int pl = lane ^ 31, sm = k / 32 - 1;
+        unsigned long long nv[S];
+        uint32_t np[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const int t = s ^ sm;
+          nv[s] = __shfl_sync(0xffffffffu, v[t], pl);
+          np[s] = __shfl_sync(0xffffffffu, p[t], pl);
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const int t = s ^ sm;
+          const bool lower = (s * 32 + lane) < (t * 32 + pl);
+          if (lower ? (nv[s] < v[s]) : (nv[s] > v[s])) {
+            v[s] = nv[s];
+            p[s] = np[s];
+          }
+        }
+      }
+    }
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void warpSortRow(uint32_t s0, uint32_t L, uint32_t r, uint32_t nx, int lane,
+                                            const unsigned long long *__restrict__ rec,
+                                            const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys,
+                                            uint32_t *__restrict__ perm) {
+  unsigned long long v[S];
+  uint32_t p[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const uint32_t e = (uint32_t)(s * 32 + lane);
+    v[s] = e < L ? rec[s0 + e] : ~0ull;
+    p[s] = e < L ? src[s0 + e] : 0u;
+  }
+  warpBitonic<S>(v, p, lane);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const uint32_t e = (uint32_t)(s * 32 + lane);
+    if (e < L) {
+      sortedKeys[s0 + e] = r * nx + (uint32_t)(v[s] >> 32);
+      perm[s0 + e] = p[s];
+    }
+  }
+}
+
+// one warp per row of <= 256 objects; longer rows go to the list of k_bucket_sort_large
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_small(
+    const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
+    const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
+    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t r = warpId; r < nRows; r += nWarps) {
+    const uint32_t s = rowStart[r], L = rowStart[r + 1] - s;
+    if (L == 0) continue;
+    if (L == 1) {
+      if (lane == 0) {
+        sortedKeys[s] = r * nx + (uint32_t)(rec[s] >> 32);
+        perm[s] = src[s];
+      }
+    } else if (L <= 32) {
+      warpSortRow<1>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+    } else if (L <= 64) {
+      warpSortRow<2>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+    } else if (L <= 128) {
+      warpSortRow<4>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+    } else if (L <= 256) {
+      warpSortRow<8>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+    } else if (lane == 0) {
+      longRows[atomicAdd(longCount, 1u)] = r;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
+    const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,
+    uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
+    const uint32_t *__restrict__ longRows, const uint32_t *__restrict__ longCount) {
+  extern __shared__ unsigned long long smem[];
+  unsigned long long *sv = smem;
+  uint32_t *sp = reinterpret_cast<uint32_t *>(smem + kLargeRow);
+  const uint32_t count = *longCount;
+  for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
+    const uint32_t r = longRows[q];
+    const uint32_t s = rowStart[r], L = rowStart[r + 1] - s;
+    uint32_t P = 1;
+    while (P < L) P <<= 1;
+    const bool inShared = L <= (uint32_t)kLargeRow;
+    unsigned long long *V = inShared ? sv : rec + s;
+    uint32_t *I = inShared ? sp : src + s;
+    if (inShared) {
+      for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+        sv[i] = rec[s + i];
+        sp[i] = src[s + i];
+      }
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+      for (uint32_t jj = k / 2; jj > 0; jj >>= 1) {
+        for (uint32_t i = threadIdx.x; i < P / 2; i += blockDim.x) {
+          uint32_t lo, hi;
+          bitonicPair(i, k, jj, lo, hi);
+          if (hi < L) {
+            const unsigned long long a = V[lo], b = V[hi];
+            if (b < a) {
+              V[lo] = b;
+              V[hi] = a;
+              const uint32_t t = I[lo];
+              I[lo] = I[hi];
+              I[hi] = t;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+      sortedKeys[s + i] = r * nx + (uint32_t)(V[i] >> 32);
+      perm[s + i] = I[i];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace ladds

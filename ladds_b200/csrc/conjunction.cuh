@@ -22,8 +22,15 @@
 
 namespace ladds {
 
+// float copy of a position with a bound on its rounding error per coordinate
+__device__ __forceinline__ float4 floatPosition(double x, double y, double z) {
+  const double m = fmax(fabs(x), fmax(fabs(y), fabs(z)));
+  return make_float4((float)x, (float)y, (float)z, (float)(m * 0x1p-22) + 1e-12f);
+}
+
 __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n,
-                          double4 *__restrict__ pos4, unsigned *__restrict__ status) {
+                          double4 *__restrict__ pos4, float4 *__restrict__ posf,
+                          unsigned *__restrict__ status) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   uint32_t p = perm[j];
@@ -35,7 +42,8 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   dst.x[j] = x;
   dst.y[j] = y;
   dst.z[j] = z;
-  pos4[j] = make_double4(x, y, z, 0.0);  // packed copy read by the candidate test
+  pos4[j] = make_double4(x, y, z, 0.0);  // packed copies read by the candidate test
+  posf[j] = floatPosition(x, y, z);
   dst.vx[j] = src.vx[p];
   dst.vy[j] = src.vy[p];
   dst.vz[j] = src.vz[p];
@@ -45,23 +53,6 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   dst.id[j] = src.id[p];
   dst.parent[j] = src.parent[p];
   dst.tag[j] = src.tag[p];
-}
-
-// rowStart[r] = lower_bound(skeys, r * nx), r in [0, nRows]
-__global__ void k_row_start(const uint32_t *__restrict__ skeys, int n, uint32_t nx, uint32_t nRows,
-                            uint32_t *__restrict__ rowStart) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r > nRows) return;
-  const uint64_t v = (uint64_t)r * nx;
-  uint32_t lo = 0, hi = (uint32_t)n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if ((uint64_t)skeys[mid] < v)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  rowStart[r] = lo;
 }
 
 __device__ __forceinline__ double dot3rn(const double a[3], const double b[3]) {
@@ -174,65 +165,6 @@ __device__ __forceinline__ void emitPair(const Obj &I, const Obj &J, double dl2,
     p.step = step;
     p.flags = flags;
     out[pos] = p;
-  }
-}
-
-__global__ void __launch_bounds__(128) k_pair_scan(DevState s, const double4 *__restrict__ pos4, int n,
-                                                   const uint32_t *__restrict__ skeys,
-                                                   const uint32_t *__restrict__ rowStart, GridDesc g, ScanConsts c,
-                                                   const int64_t *__restrict__ iterPtr, int64_t iterOffset,
-                                                   ladds_pair *__restrict__ out,
-                                                   unsigned long long *__restrict__ count, unsigned long long cap) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const int64_t it = *iterPtr + iterOffset;  // iteration index stored in the records
-  const uint32_t step = it < 0 ? 0u : (uint32_t)it;
-  const uint32_t myTag = s.tag[j];
-  if (tagDummy(myTag)) return;
-  Obj me;
-  loadObj(s, j, me);
-  const uint32_t key = skeys[j];
-  const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
-  const int32_t ix = (int32_t)(key % (uint32_t)nx);
-  const uint32_t row = key / (uint32_t)nx;
-  const int32_t iy = (int32_t)(row % (uint32_t)ny), iz = (int32_t)(row / (uint32_t)ny);
-  const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
-  for (int dz = 0; dz <= R; ++dz) {
-    const int32_t jz = iz + dz;
-    if (jz >= nz) break;
-    for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
-      const int32_t jy = iy + dy;
-      if (jy < 0 || jy >= ny) continue;
-      const uint32_t r2 = (uint32_t)jz * (uint32_t)ny + (uint32_t)jy;
-      const uint32_t rowBase = r2 * (uint32_t)nx;
-      const uint32_t end = rowStart[r2 + 1];
-      uint32_t k;
-      if (dz == 0 && dy == 0)
-        k = (uint32_t)j + 1;
-      else
-        k = lowerBound(skeys, rowStart[r2], end, rowBase + xlo);
-      const uint32_t hiKey = rowBase + xhi;
-      for (; k < end; ++k) {
-        if (skeys[k] > hiKey) break;
-        const double4 q = pos4[k];
-        const double o[3] = {q.x, q.y, q.z};
-        double d[3];
-        d[0] = __dsub_rn(me.r[0], o[0]);
-        d[1] = __dsub_rn(me.r[1], o[1]);
-        d[2] = __dsub_rn(me.r[2], o[2]);
-        const double d2 = dot3rn(d, d);  // symmetric in (i, j) bit for bit
-        if (d2 > c.cutoffSq && !nearBand(d2, c.cutoffSq, c.nearRel)) continue;
-        Obj other;
-        loadObj(s, (int)k, other);
-        if (tagDummy(other.tag)) continue;
-        const bool meFirst = me.id < other.id || (me.id == other.id && tagSlot(me.tag) < tagSlot(other.tag));
-        const Obj &I = meFirst ? me : other;
-        const Obj &J = meFirst ? other : me;
-        double dl2 = 0.0, point[3] = {0.0, 0.0, 0.0};
-        const uint32_t f = functorPair(c, I, J, d2, dl2, point);
-        if (f) emitPair(I, J, dl2, point, f, step, out, count, cap);
-      }
-    }
   }
 }
 

@@ -24,8 +24,9 @@
 
 #include "../../include/ladds_gpu.h"
 #include "conjunction.cuh"
+#include "cell_sort.cuh"
+#include "pair_scan.cuh"
 #include "propagate.cuh"
-#include "radix_sort.cuh"
 
 using namespace ladds;
 
@@ -67,7 +68,11 @@ struct ladds_gpu_ctx {
   DevState cur{}, alt{}, snap{};
   uint32_t *keys0 = nullptr, *keys1 = nullptr, *vals0 = nullptr, *vals1 = nullptr;
   uint32_t *sortedKeys = nullptr, *perm = nullptr;  // results of the last sort
-  uint32_t *counts = nullptr, *totals = nullptr;
+  unsigned long long *sortRec = nullptr;  // (ix << 32 | slot) sort records of the bucket sort
+  uint32_t *rowCounts = nullptr;          // objects per row, then the scatter cursors (2 x (nRows+1))
+  uint32_t *longRows = nullptr, *longCount = nullptr;  // rows with more than 32 objects
+  uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
+  float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
   uint32_t *rowStart = nullptr;
   uint32_t nRows = 0;
   uint32_t *scratchA = nullptr, *scratchB = nullptr, *scratchC = nullptr, *blockSums = nullptr;
@@ -75,6 +80,10 @@ struct ladds_gpu_ctx {
   ladds_pair *dPairs = nullptr;
   size_t pairCap = 0;
   unsigned long long *dCount = nullptr;
+  uint2 *dCand = nullptr;  // candidate pairs (sorted indices) of the pair scan
+  size_t candCap = 0;
+  unsigned long long *dCandCount = nullptr;  // candidates of the current scan
+  unsigned long long *dCandNeed = nullptr;   // largest candidate count of the call
   unsigned *dStatus = nullptr;
   EphEntry *dEph = nullptr;
   int64_t *dIter = nullptr;
@@ -88,6 +97,8 @@ struct ladds_gpu_ctx {
   std::map<std::tuple<int, int, int, size_t, size_t>, cudaGraphExec_t> graphs;
   std::string err;
   double *homeX = nullptr;  // x array of the buffer that was current at allocation
+  int evalBlocks = 592;     // grid of the candidate-evaluation kernel (4 per SM)
+  float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
 };
 
 namespace {
@@ -143,17 +154,21 @@ void dropGraphs(ladds_gpu_ctx *c) {
   c->graphs.clear();
 }
 
+int ensureCandCapacity(ladds_gpu_ctx *c, size_t need);
+
 void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->cur);
   freeState(c->alt);
   freeState(c->snap);
-  void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->counts, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums};
+  void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
+                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (c->pos4) cudaFree(c->pos4);
   c->pos4 = nullptr;
-  c->keys0 = c->keys1 = c->vals0 = c->vals1 = c->counts = nullptr;
+  c->posf = nullptr;
+  c->sortRec = nullptr;
+  c->scanWs = nullptr;
+  c->keys0 = c->keys1 = c->vals0 = c->vals1 = nullptr;
   c->scratchA = c->scratchB = c->scratchC = c->blockSums = nullptr;
   c->sortedKeys = c->perm = nullptr;
   c->cap = 0;
@@ -187,7 +202,6 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   c->alt = nalt;
   c->snap = nsnap;
   c->homeX = ncur.x;
-  const size_t maxTiles = (newCap + kSortTile - 1) / kSortTile;
   const size_t scanBlocks = (newCap + 1 + kScanBlock - 1) / kScanBlock;
   uint32_t **u[] = {&c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->scratchA, &c->scratchB, &c->scratchC};
   for (uint32_t **p : u) {
@@ -196,16 +210,22 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
       return fail(c, LADDS_ERR_ALLOC, "device allocation failed (sort buffers)");
     }
   }
-  if (cudaMalloc(&c->counts, (size_t)kRadix * maxTiles * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->pos4, newCap * sizeof(double4)) != cudaSuccess ||
+  // block sums of the three-level exclusive scans (objects or rows, whichever is longer)
+  const size_t scanLen = std::max(newCap + 1, (size_t)c->nRows + 1);
+  const size_t wsWords = 4 * (scanLen / kScanBlock + 2) + 4 * kScanBlock;
+  if (cudaMalloc(&c->pos4, newCap * sizeof(double4)) != cudaSuccess ||
+      cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&c->sortRec, newCap * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->blockSums, (scanBlocks + 1) * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
-    return fail(c, LADDS_ERR_ALLOC, "device allocation failed (sort counts)");
+    return fail(c, LADDS_ERR_ALLOC, "device allocation failed (cell-order buffers)");
   }
   c->cap = newCap;
   c->orderValid = false;
   dropGraphs(c);
-  return LADDS_OK;
+  // about 1.5 gated candidates per object at LEO densities; the buffer grows on overflow
+  return ensureCandCapacity(c, std::max<size_t>(2 * newCap, (size_t)1 << 16));
 }
 
 int ensurePairCapacity(ladds_gpu_ctx *c, size_t need) {
@@ -220,6 +240,40 @@ int ensurePairCapacity(ladds_gpu_ctx *c, size_t need) {
   c->dPairs = p;
   c->pairCap = newCap;
   dropGraphs(c);
+  return LADDS_OK;
+}
+
+int ensureCandCapacity(ladds_gpu_ctx *c, size_t need) {
+  if (need <= c->candCap) return LADDS_OK;
+  size_t newCap = std::max<size_t>(need + need / 2, 1);
+  uint2 *p = nullptr;
+  if (cudaMalloc(&p, newCap * sizeof(uint2)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, LADDS_ERR_ALLOC, "device allocation failed (candidate buffer)");
+  }
+  if (c->dCand) cudaFree(c->dCand);
+  c->dCand = p;
+  c->candCap = newCap;
+  dropGraphs(c);
+  return LADDS_OK;
+}
+
+// After a scan call: grows the record / candidate buffers that overflowed.
+// *overflow tells whether the call has to be re-run.
+int growIfOverflowed(ladds_gpu_ctx *c, unsigned long long *records, bool *overflow) {
+  unsigned long long cnt = 0, need = 0;
+  CK(cudaMemcpy(&cnt, c->dCount, sizeof(cnt), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&need, c->dCandNeed, sizeof(need), cudaMemcpyDeviceToHost));
+  *records = cnt;
+  *overflow = cnt > c->pairCap || need > c->candCap;
+  if (cnt > c->pairCap) {
+    const int rc = ensurePairCapacity(c, (size_t)cnt);
+    if (rc) return rc;
+  }
+  if (need > c->candCap) {
+    const int rc = ensureCandCapacity(c, (size_t)need);
+    if (rc) return rc;
+  }
   return LADDS_OK;
 }
 
@@ -292,7 +346,8 @@ cudaError_t enqueueEphemeris(ladds_gpu_ctx *c, int nSteps) {
                                  c->st);
 }
 
-void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys) {
+// nSteps steps whose stage ephemerides are c_eph[ephBase ...]
+void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
   if (c->n == 0) {
     k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
     return;
@@ -300,72 +355,111 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys) {
   PhaseScope ps(c, kPhProp);
   const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
   const int g = blocksFor(c->n, b);
+  const int n = (int)c->n;
   const bool split = c->cfg.precision == LADDS_PRECISION_SPLIT;
   if (split) {
     if (keys)
-      k_propagate<true, true><<<g, b, 0, c->st>>>(c->cur, (int)c->n, nSteps, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<true, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
     else
-      k_propagate<true, false><<<g, b, 0, c->st>>>(c->cur, (int)c->n, nSteps, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<true, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
   } else {
     if (keys)
-      k_propagate<false, true><<<g, b, 0, c->st>>>(c->cur, (int)c->n, nSteps, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<false, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
     else
-      k_propagate<false, false><<<g, b, 0, c->st>>>(c->cur, (int)c->n, nSteps, c->pc, c->grid, c->keys0,
+      k_propagate<false, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0,
                                                      c->dStatus);
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
 }
 
-// keys0 holds the keys of c->cur in current order -> sortedKeys / perm
+// exclusive scan of `count` u32 values (three levels of 1024-wide block scans,
+// count <= 2^30); block sums live in c->scanWs
+void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, uint32_t *out) {
+  const int nb1 = blocksFor(count, kScanBlock);
+  uint32_t *s1 = c->scanWs, *s1x = s1 + nb1 + 1;
+  k_scan_blocks<<<nb1, kScanBlock, 0, c->st>>>(in, (int)count, out, s1);
+  if (nb1 == 1) return;
+  const int nb2 = blocksFor((size_t)nb1, kScanBlock);
+  uint32_t *s2 = s1x + nb1 + 1;
+  k_scan_blocks<<<nb2, kScanBlock, 0, c->st>>>(s1, nb1, s1x, s2);
+  if (nb2 > 1) {
+    uint32_t *s2x = s2 + nb2 + 1, *s3 = s2x + nb2 + 1;
+    k_scan_blocks<<<1, kScanBlock, 0, c->st>>>(s2, nb2, s2x, s3);
+    k_scan_add<<<nb2, kScanBlock, 0, c->st>>>(s1x, nb1, s2x);
+  }
+  k_scan_add<<<nb1, kScanBlock, 0, c->st>>>(out, (int)count, s1x);
+}
+
+// keys0 holds the keys of c->cur in current order -> sortedKeys (keys1), perm
+// (vals1) and the row-start table; order = sort by (cell key, slot)
 void enqueueSort(ladds_gpu_ctx *c) {
   PhaseScope ps(c, kPhSort);
   const int n = (int)c->n;
-  const int numTiles = blocksFor(c->n, kSortTile);
-  const int passes = std::max(1, (int)((c->grid.keyBits + 7) / 8));
-  const uint32_t *kin = c->keys0, *vin = nullptr;
-  uint32_t *kout = c->keys1, *vout = c->vals1;
-  for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    k_radix_hist<<<numTiles, kSortThreads, 0, c->st>>>(kin, n, shift, c->counts, numTiles);
-    k_radix_scan_digit<<<kRadix, kSortThreads, 0, c->st>>>(c->counts, numTiles, c->totals);
-    k_radix_scatter<<<numTiles, kSortThreads, 0, c->st>>>(kin, vin, kout, vout, n, shift, c->counts, c->totals,
-                                                          numTiles, c->dStatus);
-    kin = kout;
-    vin = vout;
-    kout = (kout == c->keys1) ? c->keys0 : c->keys1;
-    vout = (vout == c->vals1) ? c->vals0 : c->vals1;
-  }
-  c->sortedKeys = const_cast<uint32_t *>(kin);
-  c->perm = const_cast<uint32_t *>(vin);
+  const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
+  uint32_t *rowCount = c->rowCounts, *rowCursor = c->rowCounts + nRows + 1;
+  cudaMemsetAsync(c->rowCounts, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), c->st);
+  cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
+  k_bucket_count<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(c->keys0, n, nx, rowCount);
+  enqueueExclusiveScan(c, rowCount, (size_t)nRows + 1, c->rowStart);
+  k_bucket_scatter<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
+      c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
+  const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
+  k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(c->rowStart, nRows, nx, c->sortRec, c->vals0,
+                                                                 c->keys1, c->vals1, c->longRows, c->longCount);
+  k_bucket_sort_large<<<c->evalBlocks / 2, kBucketThreads, kLargeRow * 12, c->st>>>(
+      c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount);
+  c->sortedKeys = c->keys1;
+  c->perm = c->vals1;
 }
 
 void enqueueCells(ladds_gpu_ctx *c) {
   PhaseScope ps(c, kPhCell);
-  k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, c->pos4, c->dStatus);
+  k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, c->pos4, c->posf,
+                                                      c->dStatus);
   std::swap(c->cur, c->alt);
-  k_row_start<<<blocksFor((size_t)c->nRows + 1, 256), 256, 0, c->st>>>(c->sortedKeys, (int)c->n,
-                                                                         (uint32_t)c->grid.n[0], c->nRows,
-                                                                         c->rowStart);
 }
 
 void enqueueScan(ladds_gpu_ctx *c, double dtScan, int64_t iterOffset) {
   PhaseScope ps(c, kPhScan);
   ScanConsts sc = c->sc;
   sc.dt = dtScan;
-  const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 128;
-  k_pair_scan<<<blocksFor(c->n, b), b, 0, c->st>>>(c->cur, c->pos4, (int)c->n, c->sortedKeys, c->rowStart, c->grid, sc,
-                                                    c->dIter, iterOffset, c->dPairs, c->dCount,
-                                                    (unsigned long long)c->pairCap);
+  cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), c->st);
+  k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, c->st>>>(
+      c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->grid, sc.cutoffSq, sc.nearRel,
+      c->cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
+  const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
+  // one thread per possible candidate (the count is only known on the device)
+  const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), 32768));
+  k_pair_eval<<<evalGrid, b, 0, c->st>>>(c->cur, c->dCand, c->dCandCount, (unsigned long long)c->candCap,
+                                              c->dCandNeed, sc, c->dIter, iterOffset, c->dPairs, c->dCount,
+                                              (unsigned long long)c->pairCap);
 }
 
-void enqueueIteration(ladds_gpu_ctx *c, bool scan, int k) {
-  enqueueEphemeris(c, 1);
-  enqueuePropagate(c, 1, scan);
+// one iteration; its stage ephemerides are entries 3*slot.. of the chunk table in c_eph
+void enqueueIteration(ladds_gpu_ctx *c, bool scan, int k, int slot) {
+  enqueuePropagate(c, 1, scan, 3 * slot);
   if (scan && c->n) {
     enqueueSort(c);
     enqueueCells(c);
     enqueueScan(c, c->cfg.deltaT * (double)k, -1);  // records carry the iteration just integrated
   }
+}
+
+// `len` iterations starting at iteration itStart (len <= kMaxEphSteps): one
+// ephemeris kernel + one constant-memory copy for the whole chunk.
+void enqueueChunk(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
+  enqueueEphemeris(c, len);
+  for (int i = 0; i < len; ++i) enqueueIteration(c, ((itStart + i) % k) == 0, k, i);
+}
+
+// host-side effect of replaying a captured chunk: the buffer swaps of its scans
+void replaySwaps(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
+  int scans = 0;
+  for (int i = 0; i < len; ++i) scans += ((itStart + i) % k) == 0;
+  if (!scans || !c->n) return;
+  if (scans % 2 == 1) std::swap(c->cur, c->alt);
+  c->sortedKeys = c->keys1;
+  c->perm = c->vals1;
 }
 
 int syncAndStatus(ladds_gpu_ctx *c) {
@@ -375,6 +469,7 @@ int syncAndStatus(ladds_gpu_ctx *c) {
   CK(cudaMemcpy(&status, c->dStatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
   if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
+  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait gave up (sort look-back)");
   if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
   return LADDS_OK;
 }
@@ -489,7 +584,7 @@ void ladds_gpu_config_default(ladds_gpu_config *f) {
   }
   f->device = 0;
   f->propagateBlock = 256;
-  f->scanBlock = 128;
+  f->scanBlock = 256;
   f->useGraphs = 1;
   f->pairCapacity = 0;
 }
@@ -504,7 +599,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       (f->componentMask & ~LADDS_PROP_ALL) || !(f->nearThresholdRel >= 0))
     return LADDS_ERR_INVALID_ARG;
   if (f->propagateBlock < 0 || f->propagateBlock > 256 || (f->propagateBlock % 32) || f->scanBlock < 0 ||
-      f->scanBlock > 128 || (f->scanBlock % 32))
+      f->scanBlock > 256 || (f->scanBlock % 32))
     return LADDS_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -535,11 +630,16 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   c->sc.evasionSq = f->evasionCutoff * f->evasionCutoff;
   c->sc.conjSq = f->conjunctionThreshold * f->conjunctionThreshold;
   c->sc.nearRel = f->nearThresholdRel;
+  c->cutF = (float)(f->cutoff * (1.0 + f->nearThresholdRel) * (1.0 + 1e-6));
   c->theta0 = gmstIAU1982(f->epochJD);
   if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->rowStart, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->totals, kRadix * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->rowCounts, 2 * ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->longRows, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->dCount, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dCandCount, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dStatus, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
       cudaMalloc(&c->dIter, sizeof(int64_t)) != cudaSuccess) {
@@ -552,7 +652,11 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaMemset(c->dIter, 0, sizeof(int64_t));
   cudaEventCreate(&c->callStart);
   cudaEventCreate(&c->callEnd);
+  cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
+  cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
+  c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);
+  if (!rc) rc = ensureCandCapacity(c, (size_t)1 << 16);
   if (rc) {
     ladds_gpu_destroy(c);
     return rc;
@@ -572,7 +676,8 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   dropGraphs(c);
   freeBuffers(c);
-  void *ptrs[] = {c->rowStart, c->totals, c->dCount, c->dStatus, c->dEph, c->dIter, c->dPairs};
+  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->dCount, c->dStatus, c->dEph,
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : c->events) {
@@ -752,7 +857,7 @@ int ladds_gpu_integrate(ladds_gpu_ctx *c, int steps) {
   while (left > 0) {
     const int chunk = std::min(left, kMaxEphSteps);
     CK(enqueueEphemeris(c, chunk));
-    enqueuePropagate(c, chunk, false);
+    enqueuePropagate(c, chunk, false, 0);
     left -= chunk;
   }
   const int rc = syncAndStatus(c);
@@ -769,8 +874,10 @@ int ladds_gpu_conjunctions(ladds_gpu_ctx *c, double dtScan, ladds_pair *out, siz
   CK(cudaSetDevice(c->dev));
   std::vector<ladds_pair> recs;
   if (c->n) {
-    for (int attempt = 0; attempt < 4; ++attempt) {
+    bool done = false;
+    for (int attempt = 0; attempt < 5 && !done; ++attempt) {
       CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
+      CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
       k_cell_keys<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, (int)c->n, c->grid,
                                                             c->keys0);
       enqueueSort(c);
@@ -780,15 +887,16 @@ int ladds_gpu_conjunctions(ladds_gpu_ctx *c, double dtScan, ladds_pair *out, siz
       collectTimes(c);
       if (rc) return rc;
       unsigned long long cnt = 0;
-      CK(cudaMemcpy(&cnt, c->dCount, sizeof(cnt), cudaMemcpyDeviceToHost));
-      if (cnt <= c->pairCap) {
+      bool overflow = false;
+      rc = growIfOverflowed(c, &cnt, &overflow);
+      if (rc) return rc;
+      if (!overflow) {
         recs.resize(cnt);
         if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
-        break;
+        done = true;
       }
-      rc = ensurePairCapacity(c, (size_t)cnt);
-      if (rc) return rc;
     }
+    if (!done) return fail(c, LADDS_ERR_CAPACITY, "scan buffers kept overflowing");
     c->orderValid = true;
   }
   std::sort(recs.begin(), recs.end(), pairLess);
@@ -833,33 +941,57 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
   int retries = 0;
   for (;;) {
     CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
-    CK(cudaEventRecord(c->callStart, c->st));
+    CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
     const bool graph = c->cfg.useGraphs && !c->profiling && iterations > 1;
+    const int64_t it0 = c->hostIter;
     if (graph) {
-      const auto key =
-          std::make_tuple(iterations, (int)(c->hostIter % k), c->cur.x == c->homeX ? 0 : 1, c->n, c->pairCap);
-      auto it = c->graphs.find(key);
-      if (it == c->graphs.end()) {
-        // capture performs the host-side buffer swaps of the batch
-        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < iterations; ++i) enqueueIteration(c, ((c->hostIter + i) % k) == 0, k);
-        cudaGraph_t gr = nullptr;
-        CK(cudaStreamEndCapture(c->st, &gr));
-        cudaGraphExec_t ex = nullptr;
-        const cudaError_t ie = cudaGraphInstantiate(&ex, gr, 0);
-        cudaGraphDestroy(gr);
-        CK(ie);
-        it = c->graphs.emplace(key, ex).first;
-      } else if (scans) {
-        // a replay performs the swaps of the captured batch
-        if (scans % 2 == 1) std::swap(c->cur, c->alt);
-        const int passes = std::max(1, (int)((c->grid.keyBits + 7) / 8));
-        c->sortedKeys = (passes % 2) ? c->keys1 : c->keys0;
-        c->perm = (passes % 2) ? c->vals1 : c->vals0;
+      // pass 1: capture the graphs this call needs (capture performs the host-side
+      // buffer swaps; they are undone afterwards), so that no capture happens
+      // between the timing events
+      const DevState cur0 = c->cur, alt0 = c->alt;
+      uint32_t *const sk0 = c->sortedKeys, *const pm0 = c->perm;
+      for (int done = 0; done < iterations;) {
+        const int len = std::min(iterations - done, kMaxEphSteps);
+        const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
+                                         c->pairCap);
+        if (c->graphs.find(key) == c->graphs.end()) {
+          CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+          enqueueChunk(c, it0 + done, len, k);
+          cudaGraph_t gr = nullptr;
+          CK(cudaStreamEndCapture(c->st, &gr));
+          cudaGraphExec_t ex = nullptr;
+          const cudaError_t ie = cudaGraphInstantiate(&ex, gr, 0);
+          cudaGraphDestroy(gr);
+          CK(ie);
+          c->graphs.emplace(key, ex);
+        } else {
+          replaySwaps(c, it0 + done, len, k);
+        }
+        done += len;
       }
-      CK(cudaGraphLaunch(it->second, c->st));
+      c->cur = cur0;
+      c->alt = alt0;
+      c->sortedKeys = sk0;
+      c->perm = pm0;
+      // pass 2: replay
+      CK(cudaEventRecord(c->callStart, c->st));
+      for (int done = 0; done < iterations;) {
+        const int len = std::min(iterations - done, kMaxEphSteps);
+        const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
+                                         c->pairCap);
+        auto git = c->graphs.find(key);
+        if (git == c->graphs.end()) return fail(c, LADDS_ERR_STATE, "graph cache inconsistent");
+        replaySwaps(c, it0 + done, len, k);
+        CK(cudaGraphLaunch(git->second, c->st));
+        done += len;
+      }
     } else {
-      for (int i = 0; i < iterations; ++i) enqueueIteration(c, ((c->hostIter + i) % k) == 0, k);
+      CK(cudaEventRecord(c->callStart, c->st));
+      for (int done = 0; done < iterations;) {
+        const int len = std::min(iterations - done, kMaxEphSteps);
+        enqueueChunk(c, it0 + done, len, k);
+        done += len;
+      }
     }
     CK(cudaEventRecord(c->callEnd, c->st));
     int rc = syncAndStatus(c);
@@ -868,16 +1000,19 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       const int rb = rollBack();
       return rb ? rb : rc;
     }
-    CK(cudaMemcpy(&cnt, c->dCount, sizeof(cnt), cudaMemcpyDeviceToHost));
-    if (cnt <= c->pairCap) break;
-    // device pair buffer overflowed: grow it, roll back, run the batch again
+    bool overflow = false;
+    rc = growIfOverflowed(c, &cnt, &overflow);
+    if (rc) {
+      rollBack();
+      return rc;
+    }
+    if (!overflow) break;
+    // a device record or candidate buffer overflowed: it has grown; roll back, run the batch again
     if (++retries > 4) {
       rollBack();
-      return fail(c, LADDS_ERR_CAPACITY, "device pair buffer kept overflowing");
+      return fail(c, LADDS_ERR_CAPACITY, "device scan buffers kept overflowing");
     }
     rc = rollBack();
-    if (rc) return rc;
-    rc = ensurePairCapacity(c, (size_t)cnt);
     if (rc) return rc;
   }
   float ms = 0;
@@ -977,24 +1112,9 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   k_burnup_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, c->cur.tag, n, critSq, keep,
                                                         aliveBySlot);
   // exclusive scans: positions in the current order, new slot numbers in slot order
-  auto exclusiveScan = [&](const uint32_t *in, uint32_t *outp) -> cudaError_t {
-    const int nb = blocksFor((size_t)n, kScanBlock);
-    k_scan_blocks<<<nb, kScanBlock, 0, c->st>>>(in, n, outp, c->blockSums);
-    if (nb > 1) {
-      // scan of block sums (nb <= 262144 for the 2^28 limit: two levels suffice up to 2^30)
-      uint32_t *bs2 = c->vals1;
-      const int nb2 = blocksFor((size_t)nb, kScanBlock);
-      k_scan_blocks<<<nb2, kScanBlock, 0, c->st>>>(c->blockSums, nb, c->vals0, bs2);
-      if (nb2 > 1) {
-        k_scan_blocks<<<1, kScanBlock, 0, c->st>>>(bs2, nb2, c->keys0, bs2 + nb2 + 1);
-        k_scan_add<<<nb2, kScanBlock, 0, c->st>>>(c->vals0, nb, c->keys0);
-      }
-      k_scan_add<<<nb, kScanBlock, 0, c->st>>>(outp, n, c->vals0);
-    }
-    return cudaGetLastError();
-  };
-  CK(exclusiveScan(keep, pos));
-  CK(exclusiveScan(aliveBySlot, newSlot));
+  enqueueExclusiveScan(c, keep, (size_t)n, pos);
+  enqueueExclusiveScan(c, aliveBySlot, (size_t)n, newSlot);
+  CK(cudaGetLastError());
   k_compact<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, c->alt, keep, pos, newSlot, n);
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());

@@ -42,8 +42,9 @@ __device__ __forceinline__ uint32_t cellKey(double x, double y, double z, const 
 }
 
 template <bool SPLIT, bool KEYS>
-__global__ void __launch_bounds__(256) k_propagate(DevState s, int n, int nSteps, PropConsts pc, GridDesc g,
-                                                   uint32_t *__restrict__ keys, unsigned *__restrict__ status) {
+__global__ void __launch_bounds__(256) k_propagate(DevState s, int n, int nSteps, int ephBase, PropConsts pc,
+                                                   GridDesc g, uint32_t *__restrict__ keys,
+                                                   unsigned *__restrict__ status) {
   __shared__ AtmShared atm;
   for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
     atm.h0[i] = c_atm[i].h0;
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(256) k_propagate(DevState s, int n, int nSteps
     if (tagAct(tag) == kEvasivePreserving) mask &= kPropKEP;  // Particle.h:48-52: Keplerian forces only
     double a[3];
     for (int st = 0; st < nSteps; ++st) {
-      const EphEntry *e = &c_eph[3 * st];
+      const EphEntry *e = &c_eph[ephBase + 3 * st];
 #pragma unroll
       for (int k = 0; k < 3; ++k) r[k] += pc.hc1 * v[k];
       accel<SPLIT>(mask, r, v, aom, bc, e[0], atm, a);

@@ -144,6 +144,27 @@ def test_scan_bitexact_vs_oracle(capi, oracle, cell):
     assert np.array_equal(keys, okeys[operm])
 
 
+@pytest.mark.parametrize("n,span", [(5000, 6.0), (3000, 40.0), (300, 60.0)])
+def test_cell_order_rows_of_every_length(capi, oracle, n, span):
+    """Rows of > 4096, 33-256 and <= 32 objects take different sort paths
+    (global-memory bitonic, shared-memory / multi-slot warp bitonic, one
+    register per lane); the order must equal the stable sort by key."""
+    pop = dense_population(21, n=n, span=span)
+    with ctx_for(capi, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(10.0)
+        keys, slots = ctx.cell_order()
+    opop = to_oracle(oracle, pop)
+    grid = oracle.make_grid(DENSE_BOX[0], DENSE_BOX[1], 0.0, 20.0)
+    okeys = oracle.cell_keys(opop, grid)
+    operm = oracle.stable_sort(okeys)
+    assert np.array_equal(slots, operm) and np.array_equal(keys, okeys[operm])
+    p = oracle.scan_params(cutoff=20.0, dt=10.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    ref = oracle.scan_cells(opop, p, grid)
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+
+
 def test_scan_with_deleted_objects(capi, oracle):
     pop = dense_population(12, n=3000)
     dead = np.arange(0, 3000, 7, dtype=np.uint32)
