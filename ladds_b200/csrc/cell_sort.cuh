@@ -145,7 +145,7 @@ template <int S>
 __device__ __forceinline__ void warpSortRow(uint32_t s0, uint32_t L, uint32_t r, uint32_t nx, int lane,
                                             const unsigned long long *__restrict__ rec,
                                             const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys,
-                                            uint32_t *__restrict__ perm) {
+                                            uint32_t *__restrict__ perm, uint16_t *__restrict__ sIx) {
   unsigned long long v[S];
   uint32_t p[S];
 #pragma unroll
@@ -161,44 +161,79 @@ __device__ __forceinline__ void warpSortRow(uint32_t s0, uint32_t L, uint32_t r,
     if (e < L) {
       sortedKeys[s0 + e] = r * nx + (uint32_t)(v[s] >> 32);
       perm[s0 + e] = p[s];
+      sIx[e] = (uint16_t)(v[s] >> 32);
     }
   }
 }
 
-// one warp per row of <= 256 objects; longer rows go to the list of k_bucket_sort_large
+// cellOff[c] = number of the row's objects in cells < c, c = 0..nx, from the
+// sorted cell indices ix[0..L) (one binary search per cell)
+template <typename IxAt>
+__device__ __forceinline__ void fillCellOffsets(uint16_t *__restrict__ cellOff, uint32_t nx, uint32_t L,
+                                                IxAt ixAt, uint32_t first, uint32_t stride) {
+  for (uint32_t cc = first; cc <= nx; cc += stride) {
+    uint32_t lo = 0, hi = L;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (ixAt(mid) < cc)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    cellOff[cc] = (uint16_t)lo;
+  }
+}
+
+// One warp per row of <= 256 objects; longer rows go to the list of
+// k_bucket_sort_large.  cellOff (row-major, nx + 1 entries per row; may be
+// null) receives the offset of every cell of the row inside the row.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_small(
     const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
     const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
-    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount) {
+    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff) {
+  __shared__ uint16_t sIxAll[kBucketThreads / 32][256];
   const int lane = threadIdx.x & 31;
+  uint16_t *sIx = sIxAll[threadIdx.x >> 5];
   const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t r = warpId; r < nRows; r += nWarps) {
     const uint32_t s = rowStart[r], L = rowStart[r + 1] - s;
     if (L == 0) continue;
-    if (L == 1) {
-      if (lane == 0) {
-        sortedKeys[s] = r * nx + (uint32_t)(rec[s] >> 32);
-        perm[s] = src[s];
+    if (L <= 32) {
+      // rank sort: each lane counts the smaller records (32 independent shuffles,
+      // no dependent network stages); records are unique (slot), so ranks are too
+      const unsigned long long v = lane < (int)L ? rec[s + lane] : ~0ull;
+      uint32_t rank = 0;
+#pragma unroll
+      for (int q = 0; q < 32; ++q) rank += __shfl_sync(0xffffffffu, v, q) < v ? 1u : 0u;
+      if (lane < (int)L) {
+        sortedKeys[s + rank] = r * nx + (uint32_t)(v >> 32);
+        perm[s + rank] = src[s + lane];
+        sIx[rank] = (uint16_t)(v >> 32);
       }
-    } else if (L <= 32) {
-      warpSortRow<1>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
     } else if (L <= 64) {
-      warpSortRow<2>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+      warpSortRow<2>(s, L, r, nx, lane, rec, src, sortedKeys, perm, sIx);
     } else if (L <= 128) {
-      warpSortRow<4>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
+      warpSortRow<4>(s, L, r, nx, lane, rec, src, sortedKeys, perm, sIx);
     } else if (L <= 256) {
-      warpSortRow<8>(s, L, r, nx, lane, rec, src, sortedKeys, perm);
-    } else if (lane == 0) {
-      longRows[atomicAdd(longCount, 1u)] = r;
+      warpSortRow<8>(s, L, r, nx, lane, rec, src, sortedKeys, perm, sIx);
+    } else {
+      if (lane == 0) longRows[atomicAdd(longCount, 1u)] = r;
+      continue;
     }
+    __syncwarp();
+    if (cellOff)
+      fillCellOffsets(cellOff + (size_t)r * (nx + 1), nx, L, [&](uint32_t i) { return (uint32_t)sIx[i]; },
+                      (uint32_t)lane, 32u);
+    __syncwarp();
   }
 }
 
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
     const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,
     uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
-    const uint32_t *__restrict__ longRows, const uint32_t *__restrict__ longCount) {
+    const uint32_t *__restrict__ longRows, const uint32_t *__restrict__ longCount,
+    uint16_t *__restrict__ cellOff) {
   extern __shared__ unsigned long long smem[];
   unsigned long long *sv = smem;
   uint32_t *sp = reinterpret_cast<uint32_t *>(smem + kLargeRow);
@@ -241,6 +276,9 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
       sortedKeys[s + i] = r * nx + (uint32_t)(V[i] >> 32);
       perm[s + i] = I[i];
     }
+    if (cellOff && L <= 65535u)  // offsets are 16-bit; longer rows are searched by the scan
+      fillCellOffsets(cellOff + (size_t)r * (nx + 1), nx, L, [&](uint32_t i) { return (uint32_t)(V[i] >> 32); },
+                      threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }

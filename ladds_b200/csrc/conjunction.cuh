@@ -28,8 +28,16 @@ __device__ __forceinline__ float4 floatPosition(double x, double y, double z) {
   return make_float4((float)x, (float)y, (float)z, (float)(m * 0x1p-22) + 1e-12f);
 }
 
-__global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n,
-                          double4 *__restrict__ pos4, float4 *__restrict__ posf,
+// Packed copies of the cell-ordered population read by the pair scan: one
+// 32-byte sector per load (positions + radius, velocities + id, parent + tag).
+struct ScanPack {
+  double4 *pos4;      // x, y, z, radius
+  double4 *vel4;      // vx, vy, vz, id (bit pattern)
+  ulonglong2 *meta;   // parentId, tag
+  float4 *posf;       // binary32 x, y, z + rounding bound
+};
+
+__global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n, ScanPack pk,
                           unsigned *__restrict__ status) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
@@ -39,20 +47,26 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
     p = (uint32_t)j;
   }
   const double x = src.x[p], y = src.y[p], z = src.z[p];
+  const double vx = src.vx[p], vy = src.vy[p], vz = src.vz[p];
+  const double radius = src.radius[p];
+  const uint64_t id = src.id[p], parent = src.parent[p];
+  const uint32_t tag = src.tag[p];
   dst.x[j] = x;
   dst.y[j] = y;
   dst.z[j] = z;
-  pos4[j] = make_double4(x, y, z, 0.0);  // packed copies read by the candidate test
-  posf[j] = floatPosition(x, y, z);
-  dst.vx[j] = src.vx[p];
-  dst.vy[j] = src.vy[p];
-  dst.vz[j] = src.vz[p];
+  dst.vx[j] = vx;
+  dst.vy[j] = vy;
+  dst.vz[j] = vz;
   dst.aom[j] = src.aom[p];
   dst.bc[j] = src.bc[p];
-  dst.radius[j] = src.radius[p];
-  dst.id[j] = src.id[p];
-  dst.parent[j] = src.parent[p];
-  dst.tag[j] = src.tag[p];
+  dst.radius[j] = radius;
+  dst.id[j] = id;
+  dst.parent[j] = parent;
+  dst.tag[j] = tag;
+  pk.pos4[j] = make_double4(x, y, z, radius);
+  pk.vel4[j] = make_double4(vx, vy, vz, __longlong_as_double((long long)id));
+  pk.meta[j] = make_ulonglong2(parent, tag);
+  pk.posf[j] = floatPosition(x, y, z);
 }
 
 __device__ __forceinline__ double dot3rn(const double a[3], const double b[3]) {
@@ -93,6 +107,21 @@ struct Obj {
   uint64_t id, parent;
   uint32_t tag;
 };
+
+__device__ __forceinline__ void loadObjPacked(const ScanPack &pk, uint32_t k, Obj &o) {
+  const double4 a = pk.pos4[k], b = pk.vel4[k];
+  const ulonglong2 m = pk.meta[k];
+  o.r[0] = a.x;
+  o.r[1] = a.y;
+  o.r[2] = a.z;
+  o.radius = a.w;
+  o.v[0] = b.x;
+  o.v[1] = b.y;
+  o.v[2] = b.z;
+  o.id = (uint64_t)__double_as_longlong(b.w);
+  o.parent = m.x;
+  o.tag = (uint32_t)m.y;
+}
 
 __device__ __forceinline__ void loadObj(const DevState &s, int k, Obj &o) {
   o.r[0] = s.x[k];

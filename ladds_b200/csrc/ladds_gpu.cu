@@ -70,9 +70,12 @@ struct ladds_gpu_ctx {
   uint32_t *sortedKeys = nullptr, *perm = nullptr;  // results of the last sort
   unsigned long long *sortRec = nullptr;  // (ix << 32 | slot) sort records of the bucket sort
   uint32_t *rowCounts = nullptr;          // objects per row, then the scatter cursors (2 x (nRows+1))
-  uint32_t *longRows = nullptr, *longCount = nullptr;  // rows with more than 32 objects
+  uint32_t *longRows = nullptr, *longCount = nullptr;  // rows with more than 256 objects
+  uint16_t *cellOff = nullptr;            // per row: offset of every cell inside the row (nx + 1 entries)
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
   float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
+  double4 *vel4 = nullptr;                // vx, vy, vz, id of the cell order
+  ulonglong2 *meta = nullptr;             // parentId, tag of the cell order
   uint32_t *rowStart = nullptr;
   uint32_t nRows = 0;
   uint32_t *scratchA = nullptr, *scratchB = nullptr, *scratchC = nullptr, *blockSums = nullptr;
@@ -161,11 +164,13 @@ void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->alt);
   freeState(c->snap);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs};
+                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs, c->vel4, c->meta};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c->pos4 = nullptr;
   c->posf = nullptr;
+  c->vel4 = nullptr;
+  c->meta = nullptr;
   c->sortRec = nullptr;
   c->scanWs = nullptr;
   c->keys0 = c->keys1 = c->vals0 = c->vals1 = nullptr;
@@ -215,6 +220,8 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   const size_t wsWords = 4 * (scanLen / kScanBlock + 2) + 4 * kScanBlock;
   if (cudaMalloc(&c->pos4, newCap * sizeof(double4)) != cudaSuccess ||
       cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&c->vel4, newCap * sizeof(double4)) != cudaSuccess ||
+      cudaMalloc(&c->meta, newCap * sizeof(ulonglong2)) != cudaSuccess ||
       cudaMalloc(&c->sortRec, newCap * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->blockSums, (scanBlocks + 1) * sizeof(uint32_t)) != cudaSuccess) {
@@ -404,17 +411,19 @@ void enqueueSort(ladds_gpu_ctx *c) {
   k_bucket_scatter<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
       c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
   const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
-  k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(c->rowStart, nRows, nx, c->sortRec, c->vals0,
-                                                                 c->keys1, c->vals1, c->longRows, c->longCount);
+  k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
+      c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   k_bucket_sort_large<<<c->evalBlocks / 2, kBucketThreads, kLargeRow * 12, c->st>>>(
-      c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount);
+      c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   c->sortedKeys = c->keys1;
   c->perm = c->vals1;
 }
 
+inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf}; }
+
 void enqueueCells(ladds_gpu_ctx *c) {
   PhaseScope ps(c, kPhCell);
-  k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, c->pos4, c->posf,
+  k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, scanPack(c),
                                                       c->dStatus);
   std::swap(c->cur, c->alt);
 }
@@ -425,12 +434,12 @@ void enqueueScan(ladds_gpu_ctx *c, double dtScan, int64_t iterOffset) {
   sc.dt = dtScan;
   cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), c->st);
   k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, c->st>>>(
-      c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->grid, sc.cutoffSq, sc.nearRel,
-      c->cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
+      c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
+      sc.nearRel, c->cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
   // one thread per possible candidate (the count is only known on the device)
   const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), 32768));
-  k_pair_eval<<<evalGrid, b, 0, c->st>>>(c->cur, c->dCand, c->dCandCount, (unsigned long long)c->candCap,
+  k_pair_eval<<<evalGrid, b, 0, c->st>>>(scanPack(c), c->dCand, c->dCandCount, (unsigned long long)c->candCap,
                                               c->dCandNeed, sc, c->dIter, iterOffset, c->dPairs, c->dCount,
                                               (unsigned long long)c->pairCap);
 }
@@ -654,6 +663,12 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaEventCreate(&c->callEnd);
   cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
+  // cell-offset table of the rows: used when it fits 1 GiB (250^3 cells: 31 MB)
+  const size_t cellOffBytes = (size_t)c->nRows * ((size_t)c->grid.n[0] + 1) * sizeof(uint16_t);
+  if (cellOffBytes <= ((size_t)1 << 30) && cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess) {
+    cudaGetLastError();
+    c->cellOff = nullptr;  // the scan then searches the sorted keys
+  }
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);
   if (!rc) rc = ensureCandCapacity(c, (size_t)1 << 16);
@@ -677,7 +692,7 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   dropGraphs(c);
   freeBuffers(c);
   void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->dCount, c->dStatus, c->dEph,
-                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed};
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : c->events) {
