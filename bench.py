@@ -136,16 +136,19 @@ def dist_barrier(world):
 # ----------------------------------------------------------- algorithmic work
 def algorithmic_units(n):
     """Per-step algorithmic bytes and flops of each phase (definitions in DESIGN.md)."""
-    passes = 3
     return {
         # read r, v, aom, bcInv, tag (68 B), write r, v (48 B), write the cell key (4 B)
-        "propagate": {"bytes": n * 120, "flops_fp64": None},
-        # 3 radix passes: read key (+value) for the histogram and the scatter, write key+value
-        "sort": {"bytes": n * (4 + passes * (4 + 8 + 8))},
-        # gather 92 B/object into cell order, write 92 B + 32 B packed positions, read perm
-        "cell": {"bytes": n * (92 + 92 + 32 + 4 + 4)},
-        # read own object (92 B) once; neighbours come from L2
-        "scan": {"bytes": n * 92},
+        "propagate": {"bytes": n * 120},
+        # count (key 4), scatter (key + tag 8 in, record + source 12 out)
+        "bucket": {"bytes": n * (4 + 8 + 12)},
+        # row sort: record + source in (12), sorted key + slot out (8)
+        "rowsort": {"bytes": n * (12 + 8)},
+        # gather 92 B + perm 4 into cell order; write 92 B SoA + 96 B packed + 16 B binary32 copy
+        "permute": {"bytes": n * (92 + 4 + 92 + 96 + 16)},
+        # own key, tag, pos4, posf (56 B) + ~1 candidate write (12 B)
+        "candidates": {"bytes": n * (56 + 12)},
+        # packed records of both objects of each candidate, once from DRAM (80 B per object)
+        "evaluate": {"bytes": n * 80},
     }
 
 
@@ -311,10 +314,9 @@ def main():
         ctx.set_profiling(True)
         ctx.step(min(args.steps, 64))
         pt = ctx.phase_times()
-        results[name]["phases"] = {"propagate": pt.propagateMs, "sort": pt.sortMs, "cell": pt.cellMs,
-                                   "scan": pt.scanMs, "steps": min(args.steps, 64),
-                                   "launches": {"propagate": pt.propagateLaunches, "sort": pt.sortLaunches,
-                                                "cell": pt.cellLaunches, "scan": pt.scanLaunches}}
+        results[name]["phases"] = {p: getattr(pt, p + "Ms") for p in capi.PhaseTimes.PHASES}
+        results[name]["phases"]["steps"] = min(args.steps, 64)
+        results[name]["phases"]["launches"] = {p: getattr(pt, p + "Launches") for p in capi.PhaseTimes.PHASES}
         ctx.set_profiling(False)
         ctx.close()
 
@@ -381,7 +383,7 @@ def main():
     # roofline of the dominant kernel (from the per-phase device times)
     units = algorithmic_units(n)
     ph = split["phases"]
-    per = {k: ph[k] / ph["steps"] for k in ("propagate", "sort", "cell", "scan")}
+    per = {k: ph[k] / ph["steps"] for k in capi.PhaseTimes.PHASES}
     dominant = max(per, key=per.get)
     peaks = measured_peaks_file()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
@@ -419,7 +421,8 @@ def main():
         except Exception as ex:  # noqa: BLE001
             cpu = {"value": None, "error": str(ex)[:200]}
 
-    launches_per_step = sum(split["phases"]["launches"].values()) / split["phases"]["steps"] + 1  # + k_advance
+    # kernels per step from the profiled run, + one ephemeris kernel per 128-step chunk
+    launches_per_step = sum(split["phases"]["launches"].values()) / split["phases"]["steps"]
     line = {
         "metric": METRIC,
         "value": value,
@@ -446,7 +449,7 @@ def main():
         "kernels": kernels,
         "cpu_baseline": cpu,
         "clocks": split["clocks"],
-        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "gpu_launches": int(round(launches_per_step * args.steps)) + (args.steps + 127) // 128,
         "wall_s": {"split": split["wall"], "fp64": fp64["wall"]},
     }
     print(json.dumps(line), flush=True)

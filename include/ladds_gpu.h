@@ -175,6 +175,14 @@ int ladds_gpu_integrate(ladds_gpu_ctx *ctx, int steps);
 int ladds_gpu_conjunctions(ladds_gpu_ctx *ctx, double dtScan, ladds_pair *out, size_t cap, size_t *nOut,
                            size_t *nCollisions, size_t *nEvasions, size_t *nConjunctions);
 
+/* The same scan with the functor scalars of one CollisionFunctor
+ * (CollisionFunctor.cpp:18-30): cutoff (at most the context's cutoff, which
+ * fixed the cell grid), dt, collisionDistanceFactor, minDetectionRadius,
+ * evasion cutoff, plus the conjunction threshold and near band.  Records of
+ * step index (last integrated iteration) sorted; capacity handling as above. */
+typedef struct ladds_scan_params ladds_scan_params;
+int ladds_gpu_scan(ladds_gpu_ctx *ctx, const ladds_scan_params *params, ladds_pair *out, size_t cap, size_t *nOut);
+
 /* Runs `iterations` iterations of the reference loop (Simulation.cpp:287-415):
  * integrate one step, then, when iteration % k == 0, scan with dt*k.  Records
  * of all scans are written to out (sorted).  LADDS_ERR_CAPACITY: *nOut is the
@@ -194,17 +202,52 @@ int ladds_gpu_mark_deleted(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t n);
 /* Sets every parentId to SIZE_MAX (Simulation.cpp:470-473). */
 int ladds_gpu_clear_parents(ladds_gpu_ctx *ctx);
 
+/* ---- explicit pair lists (the AoSFunctor call shape) ---- */
+/* One object of a pair evaluation (80 bytes). */
+typedef struct {
+  double r[3], v[3];  /* position [km], velocity [km/s]                   */
+  double radius;      /* [m]                                              */
+  uint64_t id;        /* Particle::getID()                                */
+  uint64_t parentId;  /* SIZE_MAX = none                                  */
+  int32_t activity;   /* LADDS_PASSIVE / LADDS_EVASIVE / ...              */
+  uint32_t slot;      /* caller's index, echoed in the record's slotA/B   */
+} ladds_object;
+
+/* Scalars of one CollisionFunctor (CollisionFunctor.cpp:18-30) plus the
+ * conjunction threshold and the near-threshold band of this library. */
+struct ladds_scan_params {
+  double cutoff, dt, collisionDistanceFactor, minDetectionRadius, evasionCutoff, conjunctionThreshold,
+      nearThresholdRel;
+};
+
+/* Evaluates CollisionFunctor::AoSFunctor(first[k], second[k]) (CollisionFunctor.cpp:
+ * 40-131) for k < nPairs on the context's device: cutoff gate, interpolation,
+ * thresholds.  Records (step 0) are sorted; *nOut = number of records; with cap
+ * too small returns LADDS_ERR_CAPACITY and *nOut = the number needed. */
+int ladds_gpu_functor_pairs(ladds_gpu_ctx *ctx, const ladds_scan_params *params, size_t nPairs,
+                            const ladds_object *first, const ladds_object *second, ladds_pair *out, size_t cap,
+                            size_t *nOut);
+
 /* Cell order of the last scan: for each sorted position its cell key and slot.
  * Used to check the sort order bit-exactly against a CPU restatement. */
 int ladds_gpu_cell_order(ladds_gpu_ctx *ctx, size_t cap, size_t *n, uint32_t *keys, uint32_t *slots);
 /* Grid actually used: cells per dimension, reach and cell size. */
 int ladds_gpu_grid(const ladds_gpu_ctx *ctx, int32_t dims[3], int32_t *reach, double *cellSize);
 
-/* Device time of the kernels of the last call, per phase [ms]: propagate,
- * sort (keys + radix passes), cell table (permute + row starts), pair scan. */
+/* Device time per phase [ms] and kernel launches per phase of the calls since
+ * ladds_gpu_set_profiling(ctx, 1) (CUDA events on the context's stream; calls
+ * then run without graphs and without overlapping scans; the per-chunk
+ * ephemeris kernel belongs to no phase):
+ *   propagate   Yoshida step + cell keys (k_propagate)
+ *   bucket      row counting sort: counts, row-start scan, scatter
+ *   rowsort     sort inside the rows + cell-offset tables
+ *   permute     gather into cell order + packed scan copies
+ *   candidates  half-shell walk, pre-filter, exact gate, compaction
+ *   evaluate    functor on the gated candidates */
 typedef struct {
-  double propagateMs, sortMs, cellMs, scanMs, totalMs;
-  uint64_t propagateLaunches, sortLaunches, cellLaunches, scanLaunches;
+  double propagateMs, bucketMs, rowsortMs, permuteMs, candidatesMs, evaluateMs, totalMs;
+  uint64_t propagateLaunches, bucketLaunches, rowsortLaunches, permuteLaunches, candidatesLaunches,
+      evaluateLaunches;
 } ladds_phase_times;
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);

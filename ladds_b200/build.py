@@ -104,10 +104,32 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
     return HOST_LIB
 
 
+HOST_TEST = os.path.join(HOST_DIR, "tests", "test_host")
+
+
+def build_host_tests(force: bool = False, verbose: bool = False) -> str:
+    """The C++ test executable of the host library (tests/test_host_cpp.py runs it)."""
+    lib = build_host(force=force, verbose=verbose)
+    src = os.path.join(HOST_DIR, "tests", "test_host.cpp")
+    if not force and _newer(HOST_TEST, [src, lib]):
+        return HOST_TEST
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    cmd = [cxx, "-std=c++17", "-O1", "-Wall", "-I", os.path.join(HOST_DIR, "include"), "-I",
+           os.path.join(ROOT, "include"), "-o", HOST_TEST, src, "-L", HOST_DIR, "-lladds_host", "-L", PKG,
+           "-lladds_gpu", f"-Wl,-rpath,{HOST_DIR}", f"-Wl,-rpath,{PKG}"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + r.stdout + r.stderr)
+    return HOST_TEST
+
+
 def build(force: bool = False, verbose: bool = False) -> None:
     build_gpu(force=force, verbose=verbose)
     build_peaks(force=force, verbose=verbose)
     build_host(force=force, verbose=verbose)
+    build_host_tests(force=force, verbose=verbose)
 
 
 if __name__ == "__main__":

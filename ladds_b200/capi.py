@@ -69,9 +69,9 @@ class StepStats(C.Structure):
 
 
 class PhaseTimes(C.Structure):
-    _fields_ = [("propagateMs", C.c_double), ("sortMs", C.c_double), ("cellMs", C.c_double), ("scanMs", C.c_double),
-                ("totalMs", C.c_double), ("propagateLaunches", C.c_uint64), ("sortLaunches", C.c_uint64),
-                ("cellLaunches", C.c_uint64), ("scanLaunches", C.c_uint64)]
+    PHASES = ("propagate", "bucket", "rowsort", "permute", "candidates", "evaluate")
+    _fields_ = ([(p + "Ms", C.c_double) for p in PHASES] + [("totalMs", C.c_double)]
+                + [(p + "Launches", C.c_uint64) for p in PHASES])
 
 
 EXPORTED = [
@@ -81,7 +81,18 @@ EXPORTED = [
     "ladds_gpu_integrate", "ladds_gpu_conjunctions", "ladds_gpu_step", "ladds_gpu_remove_below",
     "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
+    "ladds_gpu_functor_pairs", "ladds_gpu_scan",
 ]
+
+OBJECT_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("id", "<u8"),
+                         ("parentId", "<u8"), ("activity", "<i4"), ("slot", "<u4")])
+assert OBJECT_DTYPE.itemsize == 80
+
+
+class ScanParams(C.Structure):
+    _fields_ = [("cutoff", C.c_double), ("dt", C.c_double), ("collisionDistanceFactor", C.c_double),
+                ("minDetectionRadius", C.c_double), ("evasionCutoff", C.c_double),
+                ("conjunctionThreshold", C.c_double), ("nearThresholdRel", C.c_double)]
 
 _lib = None
 
@@ -122,6 +133,8 @@ def lib():
     L.ladds_gpu_set_profiling.argtypes = [vp, i]
     L.ladds_population_generate.argtypes = [i, C.c_uint64, sz] + [vp] * 12
     L.ladds_elements_to_state.argtypes = [C.c_double] * 6 + [vp, vp]
+    L.ladds_gpu_functor_pairs.argtypes = [vp, C.POINTER(ScanParams), sz, vp, vp, vp, sz, C.POINTER(sz)]
+    L.ladds_gpu_scan.argtypes = [vp, C.POINTER(ScanParams), vp, sz, C.POINTER(sz)]
     _lib = L
     return L
 
@@ -334,6 +347,34 @@ class Context:
 
     def clear_parents(self):
         self._check(self._L.ladds_gpu_clear_parents(self._h))
+
+    def scan(self, params: ScanParams, cap: int = 4096):
+        """Conjunction scan of the current state with explicit functor scalars."""
+        while True:
+            out = np.zeros(max(cap, 1), dtype=PAIR_DTYPE)
+            n = C.c_size_t()
+            rc = self._L.ladds_gpu_scan(self._h, C.byref(params), _p(out), cap, C.byref(n))
+            if rc == ERR_CAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            self._check(rc)
+            return out[: n.value].copy()
+
+    def functor_pairs(self, params: ScanParams, first: np.ndarray, second: np.ndarray):
+        """CollisionFunctor::AoSFunctor over explicit pairs (OBJECT_DTYPE arrays)."""
+        first = np.ascontiguousarray(first, dtype=OBJECT_DTYPE)
+        second = np.ascontiguousarray(second, dtype=OBJECT_DTYPE)
+        cap = max(16, len(first))
+        while True:
+            out = np.zeros(cap, dtype=PAIR_DTYPE)
+            n = C.c_size_t()
+            rc = self._L.ladds_gpu_functor_pairs(self._h, C.byref(params), len(first), _p(first), _p(second),
+                                                 _p(out), cap, C.byref(n))
+            if rc == ERR_CAPACITY:
+                cap = n.value
+                continue
+            self._check(rc)
+            return out[: n.value].copy()
 
     def set_profiling(self, on: bool):
         self._check(self._L.ladds_gpu_set_profiling(self._h, 1 if on else 0))

@@ -38,9 +38,12 @@ std::mutex g_deviceMutex[64];
 __global__ void k_advance(int64_t *iter, int by) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *iter += by;
 }
+// also stores the chunk's first iteration in *iterBase (the scans' step index)
 __global__ void k_ephemeris_dev(EphEntry *__restrict__ out, int nSteps, const int64_t *__restrict__ iterPtr,
-                                double t0, double dt, double hc1, double hc2, double jdEpoch, double theta0) {
+                                int64_t *__restrict__ iterBase, double t0, double dt, double hc1, double hc2,
+                                double jdEpoch, double theta0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *iterBase = *iterPtr;
   if (i >= 3 * nSteps) return;
   const int st = i / 3, stage = i % 3;
   const double tn = t0 + (double)(*iterPtr + st) * dt;
@@ -52,7 +55,7 @@ __global__ void k_ephemeris_dev(EphEntry *__restrict__ out, int nSteps, const in
 
 inline int blocksFor(size_t n, int b) { return (int)((n + (size_t)b - 1) / (size_t)b); }
 
-enum Phase { kPhProp = 0, kPhSort = 1, kPhCell = 2, kPhScan = 3, kPhCount = 4 };
+enum Phase { kPhProp, kPhBucket, kPhRowsort, kPhPermute, kPhCandidates, kPhEvaluate };
 
 }  // namespace
 
@@ -63,7 +66,10 @@ struct ladds_gpu_ctx {
   ScanConsts sc{};
   double theta0 = 0;
   int dev = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;   // main stream
+  cudaStream_t st2 = nullptr;  // pair scans, overlapped with the next propagation
+  cudaEvent_t evCells = nullptr, evScan = nullptr;
+  int64_t *dIterBase = nullptr;  // first iteration of the chunk being run (device)
   size_t n = 0, cap = 0;
   DevState cur{}, alt{}, snap{};
   uint32_t *keys0 = nullptr, *keys1 = nullptr, *vals0 = nullptr, *vals1 = nullptr;
@@ -93,13 +99,15 @@ struct ladds_gpu_ctx {
   int64_t hostIter = 0;
   bool orderValid = false;
   bool profiling = false;
-  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> events;
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t, int>> events;  // phase, start, end, kernels
   std::vector<cudaEvent_t> eventPool;
   ladds_phase_times times{};
   cudaEvent_t callStart = nullptr, callEnd = nullptr;
   std::map<std::tuple<int, int, int, size_t, size_t>, cudaGraphExec_t> graphs;
   std::string err;
   double *homeX = nullptr;  // x array of the buffer that was current at allocation
+  ladds_object *dObj = nullptr;  // staging of ladds_gpu_functor_pairs (2 x objCap)
+  size_t objCap = 0;
   int evalBlocks = 592;     // grid of the candidate-evaluation kernel (4 per SM)
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
 };
@@ -295,21 +303,25 @@ cudaEvent_t takeEvent(ladds_gpu_ctx *c) {
   return e;
 }
 
+// CUDA events around one phase on the stream that runs it (profiling only)
 struct PhaseScope {
   ladds_gpu_ctx *c;
   int phase;
+  cudaStream_t s;
+  int kernels;
   cudaEvent_t a = nullptr;
-  PhaseScope(ladds_gpu_ctx *c_, int ph) : c(c_), phase(ph) {
+  PhaseScope(ladds_gpu_ctx *c_, int ph, cudaStream_t s_, int kernels_ = 1)
+      : c(c_), phase(ph), s(s_), kernels(kernels_) {
     if (c->profiling) {
       a = takeEvent(c);
-      cudaEventRecord(a, c->st);
+      cudaEventRecord(a, s);
     }
   }
   ~PhaseScope() {
     if (c->profiling) {
       cudaEvent_t b = takeEvent(c);
-      cudaEventRecord(b, c->st);
-      c->events.emplace_back(phase, a, b);
+      cudaEventRecord(b, s);
+      c->events.emplace_back(phase, a, b, kernels);
     }
   }
 };
@@ -318,22 +330,32 @@ void collectTimes(ladds_gpu_ctx *c) {
   for (auto &t : c->events) {
     float ms = 0;
     cudaEventElapsedTime(&ms, std::get<1>(t), std::get<2>(t));
+    ladds_phase_times &T = c->times;
+    const int k = std::get<3>(t);
     switch (std::get<0>(t)) {
       case kPhProp:
-        c->times.propagateMs += ms;
-        c->times.propagateLaunches++;
+        T.propagateMs += ms;
+        T.propagateLaunches += k;
         break;
-      case kPhSort:
-        c->times.sortMs += ms;
-        c->times.sortLaunches++;
+      case kPhBucket:
+        T.bucketMs += ms;
+        T.bucketLaunches += k;
         break;
-      case kPhCell:
-        c->times.cellMs += ms;
-        c->times.cellLaunches++;
+      case kPhRowsort:
+        T.rowsortMs += ms;
+        T.rowsortLaunches += k;
+        break;
+      case kPhPermute:
+        T.permuteMs += ms;
+        T.permuteLaunches += k;
+        break;
+      case kPhCandidates:
+        T.candidatesMs += ms;
+        T.candidatesLaunches += k;
         break;
       default:
-        c->times.scanMs += ms;
-        c->times.scanLaunches++;
+        T.evaluateMs += ms;
+        T.evaluateLaunches += k;
         break;
     }
     c->eventPool.push_back(std::get<1>(t));
@@ -346,9 +368,9 @@ void collectTimes(ladds_gpu_ctx *c) {
 
 cudaError_t enqueueEphemeris(ladds_gpu_ctx *c, int nSteps) {
   const int threads = 3 * nSteps;
-  k_ephemeris_dev<<<blocksFor(threads, 128), 128, 0, c->st>>>(c->dEph, nSteps, c->dIter, c->cfg.startTime,
-                                                                c->cfg.deltaT, c->pc.hc1, c->pc.hc2,
-                                                                c->cfg.epochJD, c->theta0);
+  k_ephemeris_dev<<<blocksFor(threads, 128), 128, 0, c->st>>>(c->dEph, nSteps, c->dIter, c->dIterBase,
+                                                                c->cfg.startTime, c->cfg.deltaT, c->pc.hc1,
+                                                                c->pc.hc2, c->cfg.epochJD, c->theta0);
   return cudaMemcpyToSymbolAsync(c_eph, c->dEph, (size_t)threads * sizeof(EphEntry), 0, cudaMemcpyDeviceToDevice,
                                  c->st);
 }
@@ -359,7 +381,7 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
     k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
     return;
   }
-  PhaseScope ps(c, kPhProp);
+  PhaseScope ps(c, kPhProp, c->st, 2);  // propagation + iteration counter
   const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
   const int g = blocksFor(c->n, b);
   const int n = (int)c->n;
@@ -377,6 +399,13 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
                                                      c->dStatus);
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
+}
+
+// kernels launched by enqueueExclusiveScan for `count` values
+int exclusiveScanKernels(size_t count) {
+  const int nb1 = blocksFor(count, kScanBlock);
+  if (nb1 == 1) return 1;
+  return blocksFor((size_t)nb1, kScanBlock) > 1 ? 5 : 3;
 }
 
 // exclusive scan of `count` u32 values (three levels of 1024-wide block scans,
@@ -400,16 +429,19 @@ void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, ui
 // keys0 holds the keys of c->cur in current order -> sortedKeys (keys1), perm
 // (vals1) and the row-start table; order = sort by (cell key, slot)
 void enqueueSort(ladds_gpu_ctx *c) {
-  PhaseScope ps(c, kPhSort);
   const int n = (int)c->n;
   const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
   uint32_t *rowCount = c->rowCounts, *rowCursor = c->rowCounts + nRows + 1;
-  cudaMemsetAsync(c->rowCounts, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), c->st);
-  cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
-  k_bucket_count<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(c->keys0, n, nx, rowCount);
-  enqueueExclusiveScan(c, rowCount, (size_t)nRows + 1, c->rowStart);
-  k_bucket_scatter<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
-      c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
+  {
+    PhaseScope ps(c, kPhBucket, c->st, 2 + exclusiveScanKernels((size_t)nRows + 1));
+    cudaMemsetAsync(c->rowCounts, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), c->st);
+    cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
+    k_bucket_count<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(c->keys0, n, nx, rowCount);
+    enqueueExclusiveScan(c, rowCount, (size_t)nRows + 1, c->rowStart);
+    k_bucket_scatter<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
+        c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
+  }
+  PhaseScope ps(c, kPhRowsort, c->st, 2);
   const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
   k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
       c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
@@ -422,43 +454,71 @@ void enqueueSort(ladds_gpu_ctx *c) {
 inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf}; }
 
 void enqueueCells(ladds_gpu_ctx *c) {
-  PhaseScope ps(c, kPhCell);
+  PhaseScope ps(c, kPhPermute, c->st);
   k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, scanPack(c),
                                                       c->dStatus);
   std::swap(c->cur, c->alt);
 }
 
-void enqueueScan(ladds_gpu_ctx *c, double dtScan, int64_t iterOffset) {
-  PhaseScope ps(c, kPhScan);
-  ScanConsts sc = c->sc;
-  sc.dt = dtScan;
-  cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), c->st);
-  k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, c->st>>>(
-      c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
-      sc.nearRel, c->cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
+// binary32 pre-filter radius of a cutoff: cutoff * (1 + nearRel), rounded up
+inline float prefilterRadius(double cutoff, double nearRel) {
+  return (float)(cutoff * (1.0 + nearRel) * (1.0 + 1e-6));
+}
+
+// candidates + evaluation on stream s; records carry *iterPtr + iterOffset
+void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, float cutF, const int64_t *iterPtr,
+                     int64_t iterOffset) {
+  {
+    PhaseScope ps(c, kPhCandidates, s);
+    cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), s);
+    k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
+        c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
+        sc.nearRel, cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
+  }
+  PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
   // one thread per possible candidate (the count is only known on the device)
   const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), 32768));
-  k_pair_eval<<<evalGrid, b, 0, c->st>>>(scanPack(c), c->dCand, c->dCandCount, (unsigned long long)c->candCap,
-                                              c->dCandNeed, sc, c->dIter, iterOffset, c->dPairs, c->dCount,
-                                              (unsigned long long)c->pairCap);
+  k_pair_eval<<<evalGrid, b, 0, s>>>(scanPack(c), c->dCand, c->dCandCount, (unsigned long long)c->candCap,
+                                     c->dCandNeed, sc, iterPtr, iterOffset, c->dPairs, c->dCount,
+                                     (unsigned long long)c->pairCap);
 }
 
 // one iteration; its stage ephemerides are entries 3*slot.. of the chunk table in c_eph
-void enqueueIteration(ladds_gpu_ctx *c, bool scan, int k, int slot) {
-  enqueuePropagate(c, 1, scan, 3 * slot);
-  if (scan && c->n) {
-    enqueueSort(c);
-    enqueueCells(c);
-    enqueueScan(c, c->cfg.deltaT * (double)k, -1);  // records carry the iteration just integrated
-  }
-}
-
 // `len` iterations starting at iteration itStart (len <= kMaxEphSteps): one
-// ephemeris kernel + one constant-memory copy for the whole chunk.
+// ephemeris kernel + one constant-memory copy for the whole chunk.  The pair
+// scan of iteration i (candidates + evaluation) runs on the second stream,
+// concurrently with the propagation of iteration i+1: the scan reads only the
+// packed cell-order copies, the cell tables and the tags, none of which the
+// propagation writes; the next sort / gather waits for the scan.  Records
+// carry the chunk's first iteration (stored by the ephemeris kernel) + i.
 void enqueueChunk(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
   enqueueEphemeris(c, len);
-  for (int i = 0; i < len; ++i) enqueueIteration(c, ((itStart + i) % k) == 0, k, i);
+  const bool overlap = !c->profiling;
+  bool pending = false;  // a scan on the second stream that the main stream has not joined
+  for (int i = 0; i < len; ++i) {
+    const bool scan = ((itStart + i) % k) == 0 && c->n;
+    enqueuePropagate(c, 1, scan, 3 * i);
+    if (!scan) continue;
+    if (pending) {
+      cudaStreamWaitEvent(c->st, c->evScan, 0);
+      pending = false;
+    }
+    enqueueSort(c);
+    enqueueCells(c);
+    ScanConsts sc = c->sc;
+    sc.dt = c->cfg.deltaT * (double)k;
+    if (overlap) {
+      cudaEventRecord(c->evCells, c->st);
+      cudaStreamWaitEvent(c->st2, c->evCells, 0);
+      enqueueScanWith(c, c->st2, sc, c->cutF, c->dIterBase, i);
+      cudaEventRecord(c->evScan, c->st2);
+      pending = true;
+    } else {
+      enqueueScanWith(c, c->st, sc, c->cutF, c->dIterBase, i);
+    }
+  }
+  if (pending) cudaStreamWaitEvent(c->st, c->evScan, 0);
 }
 
 // host-side effect of replaying a captured chunk: the buffer swaps of its scans
@@ -651,16 +711,20 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dStatus, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
-      cudaMalloc(&c->dIter, sizeof(int64_t)) != cudaSuccess) {
+      cudaMalloc(&c->dIter, 2 * sizeof(int64_t)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     ladds_gpu_destroy(c);
     return LADDS_ERR_ALLOC;
   }
+  c->dIterBase = c->dIter + 1;
   cudaMemset(c->dStatus, 0, sizeof(unsigned));
   cudaMemset(c->dCount, 0, sizeof(unsigned long long));
-  cudaMemset(c->dIter, 0, sizeof(int64_t));
+  cudaMemset(c->dIter, 0, 2 * sizeof(int64_t));
   cudaEventCreate(&c->callStart);
   cudaEventCreate(&c->callEnd);
+  cudaEventCreateWithFlags(&c->evCells, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
   cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   // cell-offset table of the rows: used when it fits 1 GiB (250^3 cells: 31 MB)
@@ -692,7 +756,7 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   dropGraphs(c);
   freeBuffers(c);
   void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->dCount, c->dStatus, c->dEph,
-                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff};
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff, c->dObj};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : c->events) {
@@ -702,6 +766,9 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   for (auto e : c->eventPool) cudaEventDestroy(e);
   if (c->callStart) cudaEventDestroy(c->callStart);
   if (c->callEnd) cudaEventDestroy(c->callEnd);
+  if (c->evCells) cudaEventDestroy(c->evCells);
+  if (c->evScan) cudaEventDestroy(c->evScan);
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return LADDS_OK;
@@ -860,7 +927,7 @@ int ladds_gpu_set_profiling(ladds_gpu_ctx *c, int enable) {
 int ladds_gpu_phase_times(ladds_gpu_ctx *c, ladds_phase_times *t) {
   if (!c || !t) return LADDS_ERR_INVALID_ARG;
   *t = c->times;
-  t->totalMs = t->propagateMs + t->sortMs + t->cellMs + t->scanMs;
+  t->totalMs = t->propagateMs + t->bucketMs + t->rowsortMs + t->permuteMs + t->candidatesMs + t->evaluateMs;
   return LADDS_OK;
 }
 
@@ -882,39 +949,78 @@ int ladds_gpu_integrate(ladds_gpu_ctx *c, int steps) {
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+// Conjunction scan of the current state (cell keys, sort, gather, pair scan),
+// re-run with larger buffers after an overflow; sorted records in recs.
+int scanState(ladds_gpu_ctx *c, const ScanConsts &sc, float cutF, std::vector<ladds_pair> &recs) {
+  recs.clear();
+  if (!c->n) return LADDS_OK;
+  for (int attempt = 0; attempt < 5; ++attempt) {
+    CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
+    CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
+    k_cell_keys<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, (int)c->n, c->grid,
+                                                          c->keys0);
+    enqueueSort(c);
+    enqueueCells(c);
+    enqueueScanWith(c, c->st, sc, cutF, c->dIter, -1);  // records carry the index of the last integrated iteration
+    int rc = syncAndStatus(c);
+    collectTimes(c);
+    if (rc) return rc;
+    unsigned long long cnt = 0;
+    bool overflow = false;
+    rc = growIfOverflowed(c, &cnt, &overflow);
+    if (rc) return rc;
+    if (!overflow) {
+      recs.resize(cnt);
+      if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
+      c->orderValid = true;
+      std::sort(recs.begin(), recs.end(), pairLess);
+      return LADDS_OK;
+    }
+  }
+  return fail(c, LADDS_ERR_CAPACITY, "scan buffers kept overflowing");
+}
+}  // namespace
+
+extern "C" {
+
+int ladds_gpu_scan(ladds_gpu_ctx *c, const ladds_scan_params *p, ladds_pair *out, size_t cap, size_t *nOut) {
+  if (!c || !p || !nOut || !std::isfinite(p->dt) || !(p->cutoff > 0) || !(p->nearThresholdRel >= 0))
+    return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (p->cutoff > c->cfg.cutoff)
+    return fail(c, LADDS_ERR_INVALID_ARG, "scan cutoff larger than the cutoff the cell grid was built for");
+  CK(cudaSetDevice(c->dev));
+  ScanConsts sc;
+  sc.cutoffSq = p->cutoff * p->cutoff;
+  sc.dt = p->dt;
+  sc.factor = p->collisionDistanceFactor / 1000.;
+  sc.minDetectionRadius = p->minDetectionRadius;
+  sc.evasionSq = p->evasionCutoff * p->evasionCutoff;
+  sc.conjSq = p->conjunctionThreshold * p->conjunctionThreshold;
+  sc.nearRel = p->nearThresholdRel;
+  std::vector<ladds_pair> recs;
+  const int rc = scanState(c, sc, prefilterRadius(p->cutoff, p->nearThresholdRel), recs);
+  if (rc) return rc;
+  *nOut = recs.size();
+  if (recs.size() > cap || (!out && !recs.empty()))
+    return fail(c, LADDS_ERR_CAPACITY, "output buffer too small for the conjunction records");
+  if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
+  return LADDS_OK;
+}
+
 int ladds_gpu_conjunctions(ladds_gpu_ctx *c, double dtScan, ladds_pair *out, size_t cap, size_t *nOut,
                            size_t *nCollisions, size_t *nEvasions, size_t *nConjunctions) {
   if (!c || !nOut || !std::isfinite(dtScan)) return LADDS_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
   CK(cudaSetDevice(c->dev));
   std::vector<ladds_pair> recs;
-  if (c->n) {
-    bool done = false;
-    for (int attempt = 0; attempt < 5 && !done; ++attempt) {
-      CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
-      CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
-      k_cell_keys<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, (int)c->n, c->grid,
-                                                            c->keys0);
-      enqueueSort(c);
-      enqueueCells(c);
-      enqueueScan(c, dtScan, -1);  // records carry the index of the last integrated iteration
-      int rc = syncAndStatus(c);
-      collectTimes(c);
-      if (rc) return rc;
-      unsigned long long cnt = 0;
-      bool overflow = false;
-      rc = growIfOverflowed(c, &cnt, &overflow);
-      if (rc) return rc;
-      if (!overflow) {
-        recs.resize(cnt);
-        if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
-        done = true;
-      }
-    }
-    if (!done) return fail(c, LADDS_ERR_CAPACITY, "scan buffers kept overflowing");
-    c->orderValid = true;
-  }
-  std::sort(recs.begin(), recs.end(), pairLess);
+  ScanConsts sc = c->sc;
+  sc.dt = dtScan;
+  const int rc = scanState(c, sc, c->cutF, recs);
+  if (rc) return rc;
   size_t nc = 0, ne = 0, nj = 0;
   for (const auto &p : recs) {
     nc += (p.flags & LADDS_PAIR_COLLISION) != 0;
@@ -1150,6 +1256,64 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   if (nRemoved) *nRemoved = removed;
   c->orderValid = false;
   dropGraphs(c);
+  return LADDS_OK;
+}
+
+int ladds_gpu_functor_pairs(ladds_gpu_ctx *c, const ladds_scan_params *p, size_t nPairs, const ladds_object *first,
+                            const ladds_object *second, ladds_pair *out, size_t cap, size_t *nOut) {
+  if (!c || !p || !nOut || (nPairs && (!first || !second)) || nPairs > (size_t)INT32_MAX)
+    return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  *nOut = 0;
+  if (!nPairs) return LADDS_OK;
+  for (size_t k = 0; k < nPairs; ++k)
+    for (const ladds_object *o : {&first[k], &second[k]})
+      if (o->activity < 0 || o->activity > 2 || o->slot > kTagSlotMask)
+        return fail(c, LADDS_ERR_INVALID_ARG, "object activity or slot out of range");
+  CK(cudaSetDevice(c->dev));
+  if (nPairs > c->objCap) {
+    if (c->dObj) cudaFree(c->dObj);
+    c->dObj = nullptr;
+    c->objCap = 0;
+    if (cudaMalloc(&c->dObj, 2 * nPairs * sizeof(ladds_object)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(c, LADDS_ERR_ALLOC, "device allocation failed (pair objects)");
+    }
+    c->objCap = nPairs;
+  }
+  CK(cudaMemcpyAsync(c->dObj, first, nPairs * sizeof(ladds_object), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->dObj + nPairs, second, nPairs * sizeof(ladds_object), cudaMemcpyHostToDevice, c->st));
+  ScanConsts sc;
+  sc.cutoffSq = p->cutoff * p->cutoff;
+  sc.dt = p->dt;
+  sc.factor = p->collisionDistanceFactor / 1000.;
+  sc.minDetectionRadius = p->minDetectionRadius;
+  sc.evasionSq = p->evasionCutoff * p->evasionCutoff;
+  sc.conjSq = p->conjunctionThreshold * p->conjunctionThreshold;
+  sc.nearRel = p->nearThresholdRel;
+  std::vector<ladds_pair> recs;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
+    k_functor_pairs<<<blocksFor(nPairs, 256), 256, 0, c->st>>>(c->dObj, c->dObj + nPairs, (int)nPairs, sc,
+                                                                c->dPairs, c->dCount,
+                                                                (unsigned long long)c->pairCap);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    unsigned long long cnt = 0;
+    CK(cudaMemcpy(&cnt, c->dCount, sizeof(cnt), cudaMemcpyDeviceToHost));
+    if (cnt <= c->pairCap) {
+      recs.resize(cnt);
+      if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
+      break;
+    }
+    const int rc = ensurePairCapacity(c, (size_t)cnt);
+    if (rc) return rc;
+  }
+  std::sort(recs.begin(), recs.end(), pairLess);
+  *nOut = recs.size();
+  if (recs.size() > cap || (!out && !recs.empty()))
+    return fail(c, LADDS_ERR_CAPACITY, "output buffer too small for the pair records");
+  if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
   return LADDS_OK;
 }
 

@@ -171,4 +171,40 @@ __global__ void __launch_bounds__(256) k_pair_eval(ScanPack pk, const uint2 *__r
   }
 }
 
+// Explicit pair list: one thread per (first[k], second[k]).
+__global__ void __launch_bounds__(256) k_functor_pairs(const ladds_object *__restrict__ first,
+                                                       const ladds_object *__restrict__ second, int nPairs,
+                                                       ScanConsts c, ladds_pair *__restrict__ out,
+                                                       unsigned long long *__restrict__ count,
+                                                       unsigned long long cap) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nPairs) return;
+  Obj a, b;
+  const ladds_object *src[2] = {&first[q], &second[q]};
+  Obj *dst[2] = {&a, &b};
+#pragma unroll
+  for (int w = 0; w < 2; ++w) {
+    const ladds_object &o = *src[w];
+    for (int k = 0; k < 3; ++k) {
+      dst[w]->r[k] = o.r[k];
+      dst[w]->v[k] = o.v[k];
+    }
+    dst[w]->radius = o.radius;
+    dst[w]->id = o.id;
+    dst[w]->parent = o.parentId;
+    dst[w]->tag = makeTag(o.slot, o.activity, false);
+  }
+  double d[3];
+  d[0] = __dsub_rn(a.r[0], b.r[0]);
+  d[1] = __dsub_rn(a.r[1], b.r[1]);
+  d[2] = __dsub_rn(a.r[2], b.r[2]);
+  const double d2 = dot3rn(d, d);
+  const bool aFirst = a.id < b.id || (a.id == b.id && tagSlot(a.tag) < tagSlot(b.tag));
+  const Obj &I = aFirst ? a : b;
+  const Obj &J = aFirst ? b : a;
+  double dl2 = 0.0, point[3] = {0.0, 0.0, 0.0};
+  const uint32_t f = functorPair(c, I, J, d2, dl2, point);
+  if (f) emitPair(I, J, dl2, point, f, 0u, out, count, cap);
+}
+
 }  // namespace ladds

@@ -165,6 +165,60 @@ def test_cell_order_rows_of_every_length(capi, oracle, n, span):
     assert records_equal(recs, ref), describe_diff(recs, ref)
 
 
+def test_functor_pairs_vs_oracle(capi, oracle):
+    """ladds_gpu_functor_pairs (the AoSFunctor call shape) against the oracle's
+    CollisionFunctor::AoSFunctor restatement, pair by pair."""
+    rng = np.random.default_rng(31)
+    n = 4000
+    pop = dense_population(32, n=2 * n, span=30.0)
+    objs = np.zeros(2 * n, dtype=capi.OBJECT_DTYPE)
+    objs["r"] = np.stack([pop["x"], pop["y"], pop["z"]], 1)
+    objs["v"] = np.stack([pop["vx"], pop["vy"], pop["vz"]], 1)
+    objs["radius"] = pop["radius"]
+    objs["id"] = pop["id"]
+    objs["parentId"] = pop["parent"]
+    objs["activity"] = pop["activity"]
+    objs["slot"] = np.arange(2 * n)
+    first, second = objs[:n], objs[n:]
+    params = capi.ScanParams(20.0, 10.0, 2000.0, 0.05, 3.0, 2.0, 1e-9)
+    with ctx_for(capi, **DENSE_KW) as ctx:
+        recs = ctx.functor_pairs(params, first, second)
+    p = oracle.scan_params(cutoff=20.0, dt=10.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    expected = []
+    for k in range(n):
+        a, b = first[k], second[k]
+        if (int(b["id"]), int(b["slot"])) < (int(a["id"]), int(a["slot"])):
+            a, b = b, a
+        f, dl2, point = oracle.functor_pair(p, a["r"], a["v"], float(a["radius"]), int(a["activity"]),
+                                            int(a["parentId"]), b["r"], b["v"], float(b["radius"]),
+                                            int(b["activity"]), int(b["parentId"]))
+        if f:
+            expected.append((int(a["id"]), int(b["id"]), int(a["slot"]), int(b["slot"]), dl2, tuple(point), f))
+    got = [(int(r["idA"]), int(r["idB"]), int(r["slotA"]), int(r["slotB"]), float(r["dl2"]),
+            tuple(float(v) for v in r["point"]), int(r["flags"])) for r in recs]
+    key = lambda t: (t[0], t[1], t[2], t[3])
+    assert len(expected) > 50
+    assert len(got) == len(expected)
+    for g, e in zip(sorted(got, key=key), sorted(expected, key=key)):
+        assert g[:4] == e[:4] and g[6] == e[6]
+        assert (math.isnan(g[4]) and math.isnan(e[4])) or g[4] == e[4]
+        assert all((math.isnan(x) and math.isnan(y)) or x == y for x, y in zip(g[5], e[5]))
+
+
+@pytest.mark.parametrize("cutoff,conj", [(20.0, 2.0), (12.0, 0.5)])
+def test_scan_with_explicit_params(capi, oracle, cutoff, conj):
+    pop = dense_population(33, n=5000)
+    params = capi.ScanParams(cutoff, 7.0, 1500.0, 0.05, 2.0, conj, 1e-9)
+    with ctx_for(capi, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        recs = ctx.scan(params)
+    p = oracle.scan_params(cutoff=cutoff, dt=7.0, factor=1500.0, min_detection_radius=0.05, evasion_cutoff=2.0,
+                           conjunction_threshold=conj)
+    ref = oracle.scan_bruteforce(to_oracle(oracle, pop), p)
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+
+
 def test_scan_with_deleted_objects(capi, oracle):
     pop = dense_population(12, n=3000)
     dead = np.arange(0, 3000, 7, dtype=np.uint32)
