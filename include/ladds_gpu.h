@@ -44,6 +44,7 @@ extern "C" {
 #define LADDS_ERR_DEVICE_CHECK 6 /* a device-side bounds / wait check tripped        */
 #define LADDS_ERR_ALLOC 7       /* device or host allocation failed                  */
 #define LADDS_ERR_STATE 8       /* call not valid in the context's current state     */
+#define LADDS_ERR_TOO_LARGE 9   /* input beyond a fixed maximum (no-allocation call)  */
 
 /* ---- propagator components: bits 0..7 follow the reference's
  *      std::array<bool,8> order (Simulation.cpp:127-135); J3 is new. ---- */
@@ -233,6 +234,36 @@ int ladds_gpu_functor_pairs(ladds_gpu_ctx *ctx, const ladds_scan_params *params,
 int ladds_gpu_cell_order(ladds_gpu_ctx *ctx, size_t cap, size_t *n, uint32_t *keys, uint32_t *slots);
 /* Grid actually used: cells per dimension, reach and cell size. */
 int ladds_gpu_grid(const ladds_gpu_ctx *ctx, int32_t dims[3], int32_t *reach, double *cellSize);
+
+/* Cell sort that allocates nothing.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory -- processes in which another
+ * framework's caching allocator (JAX, PyTorch) has reserved nearly all of HBM,
+ * so that cudaMalloc fails, and callers on a per-iteration latency path that
+ * cannot take the implicit device synchronisation of cudaMalloc / cudaFree.
+ *
+ * keys (device, n entries): cell key (iz * ny + iy) * nx + ix of object j, as
+ * ladds_gpu_cell_order reports them; dims (host) = {nx, ny, nz}.  Writes, on
+ * `device` and `stream` (a cudaStream_t; NULL = the legacy default stream):
+ *   sortedKeys[i] (device, n)   keys in cell order,
+ *   order[i]      (device, n)   index j of the i-th object; the order is the
+ *                               sort by (key, j), the order of the contexts' scans,
+ *   rowStart      (device, ny*nz + 1 entries, may be NULL) first position of
+ *                               every cell row (iz, iy), then n.
+ * Returns once the sort has finished (it synchronises `stream`).  Its scratch
+ * is one fixed device array of about 4 MB per device, sized for at most
+ * LADDS_NOALLOC_SORT_MAX_OBJECTS objects and LADDS_NOALLOC_SORT_MAX_ROWS rows
+ * (ny * nz); larger inputs return LADDS_ERR_TOO_LARGE with a message.  Keys
+ * beyond the grid return LADDS_ERR_INVALID_ARG.  The first call on a device
+ * looks up the array's device address (set-up, once per device); make that
+ * first call before any stream capture.  Every call shares the array, which
+ * keeps the last call's contents: calls that overlap on the GPU (other streams
+ * or host threads, same device) race.  errMsg (may be NULL) receives a
+ * message of at most errMsgCap bytes, "" on success. */
+#define LADDS_NOALLOC_SORT_MAX_OBJECTS 262144
+#define LADDS_NOALLOC_SORT_MAX_ROWS 65536
+int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, size_t n, const int32_t dims[3],
+                                uint32_t *sortedKeys, uint32_t *order, uint32_t *rowStart, char *errMsg,
+                                size_t errMsgCap);
 
 /* Device time per phase [ms] and kernel launches per phase of the calls since
  * ladds_gpu_set_profiling(ctx, 1) (CUDA events on the context's stream; calls

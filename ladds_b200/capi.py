@@ -16,8 +16,9 @@ import numpy as np
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libladds_gpu.so")
 
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_CAPACITY, ERR_NONFINITE, ERR_NO_DEVICE, ERR_DEVICE_CHECK, ERR_ALLOC, ERR_STATE = \
-    range(9)
+(OK, ERR_INVALID_ARG, ERR_CUDA, ERR_CAPACITY, ERR_NONFINITE, ERR_NO_DEVICE, ERR_DEVICE_CHECK, ERR_ALLOC, ERR_STATE,
+ ERR_TOO_LARGE) = range(10)
+NOALLOC_SORT_MAX_OBJECTS, NOALLOC_SORT_MAX_ROWS = 262144, 65536
 KEP, J2, C22, S22, SOL, LUN, SRP, DRAG, J3 = (1 << k for k in range(9))
 PROP_ALL = 0x1FF
 PASSIVE, EVASIVE, EVASIVE_PRESERVING = 0, 1, 2
@@ -81,7 +82,7 @@ EXPORTED = [
     "ladds_gpu_integrate", "ladds_gpu_conjunctions", "ladds_gpu_step", "ladds_gpu_remove_below",
     "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
-    "ladds_gpu_functor_pairs", "ladds_gpu_scan",
+    "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc",
 ]
 
 OBJECT_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("id", "<u8"),
@@ -135,6 +136,7 @@ def lib():
     L.ladds_elements_to_state.argtypes = [C.c_double] * 6 + [vp, vp]
     L.ladds_gpu_functor_pairs.argtypes = [vp, C.POINTER(ScanParams), sz, vp, vp, vp, sz, C.POINTER(sz)]
     L.ladds_gpu_scan.argtypes = [vp, C.POINTER(ScanParams), vp, sz, C.POINTER(sz)]
+    L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
     return L
 

@@ -1318,3 +1318,212 @@ int ladds_gpu_functor_pairs(ladds_gpu_ctx *c, const ladds_scan_params *p, size_t
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Cell sort without allocation (ladds_gpu_cell_sort_noalloc).
+//
+// For callers that cannot allocate device memory: processes in which another
+// framework's caching allocator (JAX, PyTorch) has reserved nearly all of HBM,
+// so that cudaMalloc fails, and callers on a per-iteration latency path that
+// cannot take the implicit device synchronisation of cudaMalloc / cudaFree.
+// All scratch of the sort (row counts and cursors, row-start table, sort
+// records, source indices, long-row list, scan partial sums, status word)
+// lives in one file-scope device array of fixed size; the caller supplies the
+// keys and the output buffers.  Every call shares the array and it keeps the
+// last call's contents, so each call clears what must start at zero, and calls
+// that overlap on the GPU (other streams, other host threads) race.
+namespace {
+
+constexpr size_t naRound(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kNaMaxObjects = LADDS_NOALLOC_SORT_MAX_OBJECTS;
+constexpr size_t kNaMaxRows = LADDS_NOALLOC_SORT_MAX_ROWS;
+constexpr size_t kNaScanBlocks = (kNaMaxRows + 1 + kScanBlock - 1) / kScanBlock;
+static_assert(kNaScanBlocks <= (size_t)kScanBlock, "two scan levels must cover the row table");
+// byte offsets inside the scratch array
+constexpr size_t kNaRec = 0;                                                   // u64 per object
+constexpr size_t kNaSrc = kNaRec + naRound(8 * kNaMaxObjects);                 // u32 per object
+constexpr size_t kNaCounts = kNaSrc + naRound(4 * kNaMaxObjects);              // counts | cursors
+constexpr size_t kNaRowStart = kNaCounts + naRound(8 * (kNaMaxRows + 1));      // u32 per row + 1
+constexpr size_t kNaLong = kNaRowStart + naRound(4 * (kNaMaxRows + 1));        // long-row list
+constexpr size_t kNaMisc = kNaLong + naRound(4 * kNaMaxRows);                  // longCount, status
+constexpr size_t kNaScan = kNaMisc + 256;                                      // scan partial sums
+constexpr size_t kNaBytes = kNaScan + naRound(4 * (2 * (kNaScanBlocks + 1) + 2));
+
+static __device__ __align__(256) unsigned char g_noallocSortScratch[kNaBytes];
+
+struct NaDevice {
+  unsigned char *scratch = nullptr;  // device address of g_noallocSortScratch on this device
+  int sms = 0;
+};
+NaDevice g_naDevice[64];
+std::mutex g_naMutex;
+
+void naMessage(char *msg, size_t cap, const char *text) {
+  if (msg && cap) std::snprintf(msg, cap, "%s", text);
+}
+
+// status bits: 1 = a key beyond the grid, 2 = inconsistent row counts
+__global__ void __launch_bounds__(kBucketThreads) k_na_count(const uint32_t *__restrict__ keys, int n, uint32_t nx,
+                                                             uint32_t nRows, uint32_t *__restrict__ rowCount,
+                                                             unsigned *__restrict__ status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t row = 0xffffffffu;
+  if (j < n) {
+    row = keys[j] / nx;
+    if (row >= nRows) {
+      atomicOr(status, 1u);
+      row = 0xffffffffu;
+    }
+  }
+  const bool valid = row != 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, row);
+  if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&rowCount[row], (uint32_t)__popc(peers));
+}
+
+// sort record ix << 32 | j and source j of every object j (the index in keys)
+__global__ void __launch_bounds__(kBucketThreads) k_na_scatter(const uint32_t *__restrict__ keys, int n, uint32_t nx,
+                                                               uint32_t nRows, const uint32_t *__restrict__ rowStart,
+                                                               uint32_t *__restrict__ rowCursor,
+                                                               unsigned long long *__restrict__ rec,
+                                                               uint32_t *__restrict__ src,
+                                                               unsigned *__restrict__ status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const uint32_t key = j < n ? keys[j] : 0u;
+  uint32_t row = j < n ? key / nx : 0xffffffffu;
+  if (row >= nRows) row = 0xffffffffu;  // counted as an error by k_na_count
+  const bool valid = row != 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, row);
+  const int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (valid && lane == leader) base = atomicAdd(&rowCursor[row], (uint32_t)__popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!valid) return;
+  const uint32_t pos = rowStart[row] + base + (uint32_t)__popc(peers & laneMaskLt());
+  if (pos >= rowStart[row + 1]) {
+    atomicOr(status, 2u);
+    return;
+  }
+  rec[pos] = ((unsigned long long)(key - row * nx) << 32) | (uint32_t)j;
+  src[pos] = (uint32_t)j;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t status;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    status = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, size_t n, const int32_t dims[3],
+                                uint32_t *sortedKeys, uint32_t *order, uint32_t *rowStart, char *errMsg,
+                                size_t errMsgCap) {
+  naMessage(errMsg, errMsgCap, "");
+  if (!dims || device < 0 || device >= 64 || (n && (!keys || !sortedKeys || !order))) {
+    naMessage(errMsg, errMsgCap, "invalid argument: null pointer or device index");
+    return LADDS_ERR_INVALID_ARG;
+  }
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 ||
+      (uint64_t)dims[0] * (uint64_t)dims[1] * (uint64_t)dims[2] > (1ull << 32)) {
+    naMessage(errMsg, errMsgCap, "invalid argument: grid dimensions must be >= 1 with at most 2^32 cells");
+    return LADDS_ERR_INVALID_ARG;
+  }
+  const uint64_t nRows64 = (uint64_t)dims[1] * (uint64_t)dims[2];
+  if (n > kNaMaxObjects || nRows64 > kNaMaxRows) {
+    char text[160];
+    std::snprintf(text, sizeof(text),
+                  "too large: %zu objects and %llu cell rows exceed the fixed scratch maximum of %zu objects / "
+                  "%zu rows",
+                  n, (unsigned long long)nRows64, kNaMaxObjects, kNaMaxRows);
+    naMessage(errMsg, errMsgCap, text);
+    return LADDS_ERR_TOO_LARGE;
+  }
+  DeviceGuard guard(device);
+  if (guard.status != cudaSuccess) {
+    cudaGetLastError();
+    naMessage(errMsg, errMsgCap, cudaGetErrorString(guard.status));
+    return guard.status == cudaErrorInvalidDevice || guard.status == cudaErrorNoDevice ? LADDS_ERR_NO_DEVICE
+                                                                                        : LADDS_ERR_CUDA;
+  }
+  NaDevice &d = g_naDevice[device];
+  {
+    std::lock_guard<std::mutex> lk(g_naMutex);
+    if (!d.scratch) {  // set-up, once per device, with that device current
+      int sms = 0;
+      unsigned char *ptr = nullptr;
+      const cudaError_t e1 = cudaGetSymbolAddress((void **)&ptr, g_noallocSortScratch);
+      const cudaError_t e2 = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+      if (e1 != cudaSuccess || e2 != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        naMessage(errMsg, errMsgCap, cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        return LADDS_ERR_CUDA;
+      }
+      d.sms = std::max(sms, 1);
+      d.scratch = ptr;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t nx = (uint32_t)dims[0], nRows = (uint32_t)nRows64;
+  auto *rec = reinterpret_cast<unsigned long long *>(d.scratch + kNaRec);
+  auto *src = reinterpret_cast<uint32_t *>(d.scratch + kNaSrc);
+  auto *rowCount = reinterpret_cast<uint32_t *>(d.scratch + kNaCounts);
+  uint32_t *rowCursor = rowCount + nRows + 1;
+  auto *rowStartS = reinterpret_cast<uint32_t *>(d.scratch + kNaRowStart);
+  auto *longRows = reinterpret_cast<uint32_t *>(d.scratch + kNaLong);
+  auto *longCount = reinterpret_cast<uint32_t *>(d.scratch + kNaMisc);
+  auto *status = reinterpret_cast<unsigned *>(d.scratch + kNaMisc + 4);
+  auto *s1 = reinterpret_cast<uint32_t *>(d.scratch + kNaScan);
+  uint32_t *s1x = s1 + kNaScanBlocks + 1, *s2 = s1x + kNaScanBlocks + 1;
+
+  cudaMemsetAsync(rowCount, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), s);
+  cudaMemsetAsync(longCount, 0, 2 * sizeof(uint32_t), s);  // longCount and status
+  if (n) {
+    const int gridN = blocksFor(n, kBucketThreads);
+    k_na_count<<<gridN, kBucketThreads, 0, s>>>(keys, (int)n, nx, nRows, rowCount, status);
+  }
+  const size_t count = (size_t)nRows + 1;
+  const int nb1 = blocksFor(count, kScanBlock);
+  k_scan_blocks<<<nb1, kScanBlock, 0, s>>>(rowCount, (int)count, rowStartS, s1);
+  if (nb1 > 1) {
+    k_scan_blocks<<<1, kScanBlock, 0, s>>>(s1, nb1, s1x, s2);
+    k_scan_add<<<nb1, kScanBlock, 0, s>>>(rowStartS, (int)count, s1x);
+  }
+  if (n) {
+    const int gridN = blocksFor(n, kBucketThreads);
+    k_na_scatter<<<gridN, kBucketThreads, 0, s>>>(keys, (int)n, nx, nRows, rowStartS, rowCursor, rec, src, status);
+    const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 64 * d.sms);
+    k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, s>>>(rowStartS, nRows, nx, rec, src, sortedKeys, order,
+                                                               longRows, longCount, nullptr);
+    k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(rowStartS, nx, rec, src, sortedKeys,
+                                                                          order, longRows, longCount, nullptr);
+  }
+  if (rowStart) cudaMemcpyAsync(rowStart, rowStartS, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+  unsigned hostStatus = 0;
+  cudaMemcpyAsync(&hostStatus, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    naMessage(errMsg, errMsgCap, cudaGetErrorString(e));
+    return LADDS_ERR_CUDA;
+  }
+  if (hostStatus & 1u) {
+    naMessage(errMsg, errMsgCap, "invalid argument: a key lies beyond the grid (key >= dims[0]*dims[1]*dims[2])");
+    return LADDS_ERR_INVALID_ARG;
+  }
+  if (hostStatus) {
+    naMessage(errMsg, errMsgCap, "device check: inconsistent row counts");
+    return LADDS_ERR_DEVICE_CHECK;
+  }
+  return LADDS_OK;
+}
+
+}  // extern "C"
