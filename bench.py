@@ -152,6 +152,20 @@ def algorithmic_units(n):
     }
 
 
+def profiled_traffic(n):
+    """DRAM bytes per launch of each phase's main kernel from the committed ncu
+    summary (1e6 objects), scaled to n objects."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "dram_traffic_population0_1e6.txt")):
+            if line.strip() and not line.startswith("#"):
+                phase, _, nbytes = line.split()
+                out[phase] = int(nbytes) * n / 1e6
+    except (OSError, ValueError):
+        pass
+    return out
+
+
 def propagation_flops(mask_full=True):
     # counted FP operations per force evaluation of the restated model (DESIGN.md)
     f_eval = 208 if mask_full else 33
@@ -402,8 +416,11 @@ def main():
     if f64_peak:
         kernels["propagate_fp64_mode"]["fp64_frac"] = kernels["propagate_fp64_mode"]["achieved_tflops"] / f64_peak
     dk = kernels[dominant]
+    traffic = profiled_traffic(n).get(dominant)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["achieved_gbs"], "peak": hbm_peak,
-                "unit": "GB/s", "frac": dk["hbm_frac"], "traffic": None,
+                "unit": "GB/s", "frac": dk["hbm_frac"], "traffic": traffic,
+                "traffic_source": "profiles/dram_traffic_population0_1e6.txt (one ncu capture, scaled by n/1e6)"
+                if traffic else None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
 
     cpu = None
