@@ -278,6 +278,56 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------- adjoint leg
+def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
+    """Differentiation workload: 4096 pairs, 1080 FP64 steps of the full force
+    set, checkpoints every 64 steps.  Device times of the forward sweep (loss +
+    checkpoints) and of the backward sweep (segment recompute + reverse sweep),
+    and a directional central-difference check of every pair's gradient
+    (Richardson-extrapolated from eps and eps / 2, eps = 1e-6 |x|)."""
+    with capi.Context(capi.default_config(componentMask=capi.PROP_ALL, device=device)) as ctx:
+        pairs, _ = ctx.adjoint_make_pairs(77, n_pairs, steps)
+        ctx.adjoint_forward(pairs, steps, ck)
+        ctx.adjoint_backward()
+        fwd, bwd = [], []
+        for _ in range(reps):
+            fwd.append(ctx.adjoint_forward(pairs, steps, ck)[3])
+            dx, _, ms = ctx.adjoint_backward()
+            bwd.append(ms)
+        rows = np.concatenate([pairs["rA"], pairs["vA"], pairs["rB"], pairs["vB"]], axis=1)
+        rng = np.random.default_rng(3)
+        d = rng.normal(size=rows.shape) * np.abs(rows)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        eps = 1e-6 * np.linalg.norm(rows, axis=1)
+        batch = []
+        for f in (1.0, -1.0, 0.5, -0.5):
+            q = pairs.copy()
+            r = rows + f * eps[:, None] * d
+            q["rA"], q["vA"], q["rB"], q["vB"] = r[:, 0:3], r[:, 3:6], r[:, 6:9], r[:, 9:12]
+            batch.append(q)
+        _, miss, stepP, _ = ctx.adjoint_forward(np.concatenate(batch), steps, ck)
+        step0 = ctx.adjoint_forward(pairs, steps, ck)[2]
+    miss = miss.reshape(4, n_pairs)
+    smooth = np.all(stepP.reshape(4, n_pairs) == step0[None, :], axis=0)  # the stencil keeps the argmin
+    fd1 = (miss[0] - miss[1]) / (2 * eps)
+    fd2 = (miss[2] - miss[3]) / eps
+    rich = (4.0 * fd2 - fd1) / 3.0
+    gd = np.sum(dx * d, axis=1)
+    rel = (np.abs(gd - rich) / np.abs(rich))[smooth]
+    rel1 = (np.abs(gd - fd1) / np.abs(fd1))[smooth]
+    f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    return {"pairs": n_pairs, "steps": steps, "checkpoint_every": ck, "forward_ms": f_ms, "backward_ms": b_ms,
+            "backward_over_forward": b_ms / f_ms, "forward_plus_backward_over_forward": (f_ms + b_ms) / f_ms,
+            "fd_check": {"direction": "random per pair, 12 state components, relative scaling",
+                         "pairs_checked": int(np.sum(smooth)),
+                         "pairs_skipped_argmin_switch": int(np.sum(~smooth)),
+                         "nonfinite": int(np.sum(~np.isfinite(rel))),
+                         "richardson_rel_err_median": float(np.nanmedian(rel)),
+                         "richardson_rel_err_p99": float(np.nanquantile(rel, 0.99)),
+                         "central_h1e-6_rel_err_median": float(np.nanmedian(rel1)),
+                         "central_h1e-6_rel_err_p99": float(np.nanquantile(rel1, 0.99))}}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -289,6 +339,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--no-drift", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--reference-budget", type=float, default=150.0)
     args = ap.parse_args()
@@ -335,6 +386,14 @@ def main():
         ctx.close()
 
     # one-day drift of split vs FP64 (both from the same start state)
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        try:
+            adjoint = adjoint_leg(capi, local)
+        except Exception as ex:  # noqa: BLE001
+            adjoint = {"error": str(ex)[:200]}
+            print(f"adjoint leg failed: {ex}", file=sys.stderr)
+
     drift = None
     if not args.no_drift and rank == 0:
         finals = {}
@@ -459,7 +518,8 @@ def main():
         "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
         "mixed_over_fp64": value / fp64_value,
         "drift": drift,
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
+        "adjoint": adjoint,
         "records": {"split": split["records"], "fp64": fp64["records"]},
         "e2e": e2e,
         "roofline": roofline,

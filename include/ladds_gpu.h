@@ -283,6 +283,40 @@ typedef struct {
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
 
+/* ---- adjoint of the propagation for conjunction pairs ----
+ * Loss of a batch of pairs (A_p, B_p) propagated independently from the
+ * context's startTime with its deltaT and component mask, FP64:
+ *   L = sum_p min_{s=1..steps} dl2_p(s),
+ * dl2_p(s) = the squared miss distance of the pair over step s (the linear
+ * interpolation of DistanceApproximation.cpp:13-58 as used by
+ * CollisionFunctor.cpp:94-129, i = A, j = B).  The reference has no
+ * differentiation; the pair is the AoSFunctor pair after `steps` integrate(false)
+ * calls (Simulation.cpp:297).  Pairs whose dl2 is NaN at every step add
+ * nothing and get a zero gradient (tcaStep 0). */
+typedef struct {
+  double rA[3], vA[3], rB[3], vB[3]; /* km, km/s at the start time */
+  double bcInvA, bcInvB;             /* Cd A / m [m^2/kg] (Particle.cpp:13-27) */
+  double aomA, aomB;                 /* pi r^2 1e-6 / m [km^2/kg] (Particle.h:72) */
+} ladds_adjoint_pair;
+
+/* Forward sweep: the loss, per-pair min dl2 (missSq) and its step (tcaStep,
+ * 1-based), both may be NULL; stores the states every checkpointEvery steps on
+ * the device for the backward sweep.  deviceMs (may be NULL): kernel time. */
+int ladds_gpu_adjoint_forward(ladds_gpu_ctx *ctx, const ladds_adjoint_pair *pairs, size_t nPairs, int steps,
+                              int checkpointEvery, double *missSq, int32_t *tcaStep, double *loss,
+                              double *deviceMs);
+/* Backward sweep of the last forward sweep (segments recomputed from the
+ * checkpoints): dL_dx0[12 p ..] = dL/d(rA, vA, rB, vB), dL_dbc[2 p ..] =
+ * dL/d(bcInvA, bcInvB).  LADDS_ERR_STATE without a preceding forward sweep. */
+int ladds_gpu_adjoint_backward(ladds_gpu_ctx *ctx, double *dL_dx0, double *dL_dbc, double *deviceMs);
+/* Synthetic pairs of the differentiation benchmark: A and B from population 0
+ * (objects 2p, 2p + 1 of `seed`); B is placed at A's state after
+ * tcaStep = round(1.5 T_A / dt) steps (<= steps - 1) plus an offset of
+ * U[0.05, 2] km and U[0.01, 0.5] km/s in random directions, then propagated
+ * back to the start with the FP64 path.  tcaStep may be NULL. */
+int ladds_gpu_adjoint_make_pairs(ladds_gpu_ctx *ctx, uint64_t seed, size_t nPairs, int steps,
+                                 ladds_adjoint_pair *out, int32_t *tcaStep);
+
 /* ---- synthetic populations (host) ---- */
 /* Fills SoA arrays with population `which` of the benchmark definitions:
  *  0: N objects, a = R + U[400,1500] km, e U[0,0.02], i U[0,180] deg, RAAN /

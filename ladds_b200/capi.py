@@ -82,8 +82,13 @@ EXPORTED = [
     "ladds_gpu_integrate", "ladds_gpu_conjunctions", "ladds_gpu_step", "ladds_gpu_remove_below",
     "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
-    "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc",
+    "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
+    "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs",
 ]
+
+ADJ_PAIR_DTYPE = np.dtype([("rA", "<f8", (3,)), ("vA", "<f8", (3,)), ("rB", "<f8", (3,)), ("vB", "<f8", (3,)),
+                           ("bcInvA", "<f8"), ("bcInvB", "<f8"), ("aomA", "<f8"), ("aomB", "<f8")])
+assert ADJ_PAIR_DTYPE.itemsize == 128
 
 OBJECT_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("id", "<u8"),
                          ("parentId", "<u8"), ("activity", "<i4"), ("slot", "<u4")])
@@ -136,6 +141,9 @@ def lib():
     L.ladds_elements_to_state.argtypes = [C.c_double] * 6 + [vp, vp]
     L.ladds_gpu_functor_pairs.argtypes = [vp, C.POINTER(ScanParams), sz, vp, vp, vp, sz, C.POINTER(sz)]
     L.ladds_gpu_scan.argtypes = [vp, C.POINTER(ScanParams), vp, sz, C.POINTER(sz)]
+    L.ladds_gpu_adjoint_forward.argtypes = [vp, vp, sz, i, i, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.ladds_gpu_adjoint_backward.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
+    L.ladds_gpu_adjoint_make_pairs.argtypes = [vp, C.c_uint64, sz, i, vp, vp]
     L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
     return L
@@ -377,6 +385,35 @@ class Context:
                 continue
             self._check(rc)
             return out[: n.value].copy()
+
+    # ---- adjoint of the propagation for conjunction pairs
+    def adjoint_make_pairs(self, seed: int, n_pairs: int, steps: int):
+        """Synthetic pairs of the differentiation benchmark; returns (pairs, tca)."""
+        pairs = np.zeros(n_pairs, dtype=ADJ_PAIR_DTYPE)
+        tca = np.zeros(n_pairs, dtype=np.int32)
+        self._check(self._L.ladds_gpu_adjoint_make_pairs(self._h, seed, n_pairs, steps, _p(pairs), _p(tca)))
+        return pairs, tca
+
+    def adjoint_forward(self, pairs: np.ndarray, steps: int, checkpoint_every: int = 64):
+        """Loss sum_p min_s dl2; returns (loss, missSq, tcaStep, device ms)."""
+        pairs = np.ascontiguousarray(pairs, dtype=ADJ_PAIR_DTYPE)
+        n = len(pairs)
+        miss = np.zeros(n, dtype=np.float64)
+        tca = np.zeros(n, dtype=np.int32)
+        loss, ms = C.c_double(), C.c_double()
+        self._check(self._L.ladds_gpu_adjoint_forward(self._h, _p(pairs), n, steps, checkpoint_every, _p(miss),
+                                                      _p(tca), C.byref(loss), C.byref(ms)))
+        self._adj_n = n
+        return loss.value, miss, tca, ms.value
+
+    def adjoint_backward(self):
+        """Gradients of the last forward sweep: (dL/d(rA, vA, rB, vB) [P, 12], dL/d(bcA, bcB) [P, 2], ms)."""
+        n = getattr(self, "_adj_n", 0)
+        dx = np.zeros((max(n, 1), 12), dtype=np.float64)
+        dbc = np.zeros((max(n, 1), 2), dtype=np.float64)
+        ms = C.c_double()
+        self._check(self._L.ladds_gpu_adjoint_backward(self._h, _p(dx), _p(dbc), C.byref(ms)))
+        return dx[:n], dbc[:n], ms.value
 
     def set_profiling(self, on: bool):
         self._check(self._L.ladds_gpu_set_profiling(self._h, 1 if on else 0))

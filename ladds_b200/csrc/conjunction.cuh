@@ -75,8 +75,9 @@ __device__ __forceinline__ double dot3rn(const double a[3], const double b[3]) {
   return __dadd_rn(r, __dmul_rn(a[2], b[2]));
 }
 
-// distanceByLinearInterpolation (DistanceApproximation.cpp:13-58)
-__device__ __forceinline__ void interpolate(const double ri[3], const double vi[3], const double rj[3],
+// distanceByLinearInterpolation (DistanceApproximation.cpp:13-58); returns the
+// clamped closest-approach parameter t in [0, dt] (measured from r - v dt)
+__device__ __forceinline__ double interpolate(const double ri[3], const double vi[3], const double rj[3],
                                             const double vj[3], double dt, double dr[3], double p2[3]) {
   double oi[3], oj[3];
 #pragma unroll
@@ -96,6 +97,7 @@ __device__ __forceinline__ void interpolate(const double ri[3], const double vi[
     p2[k] = __dadd_rn(oj[k], __dmul_rn(vj[k], t));
     dr[k] = __dsub_rn(p1, p2[k]);
   }
+  return t;
 }
 
 __device__ __forceinline__ bool nearBand(double x, double thr2, double rel) {

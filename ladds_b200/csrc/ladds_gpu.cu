@@ -27,6 +27,8 @@
 #include "cell_sort.cuh"
 #include "pair_scan.cuh"
 #include "propagate.cuh"
+#include "adjoint.cuh"
+#include "population.h"
 
 using namespace ladds;
 
@@ -110,6 +112,16 @@ struct ladds_gpu_ctx {
   size_t objCap = 0;
   int evalBlocks = 592;     // grid of the candidate-evaluation kernel (4 per SM)
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
+  struct Adjoint {          // buffers of the adjoint pair batch (ladds_gpu_adjoint_*)
+    size_t nPairs = 0;
+    int steps = 0, ck = 0;
+    bool forwardDone = false;
+    double *st = nullptr, *bc = nullptr, *aom = nullptr, *miss = nullptr, *grad = nullptr;
+    double *ckpt = nullptr, *rec = nullptr, *off = nullptr;
+    int *arg = nullptr;
+    EphEntry *eph = nullptr;
+    size_t objCap = 0, ckptCap = 0, recCap = 0, ephCap = 0;
+  } adj;
 };
 
 namespace {
@@ -756,7 +768,9 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   dropGraphs(c);
   freeBuffers(c);
   void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->dCount, c->dStatus, c->dEph,
-                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff, c->dObj};
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff, c->dObj,
+                  c->adj.st, c->adj.bc, c->adj.aom, c->adj.miss, c->adj.grad, c->adj.ckpt, c->adj.rec,
+                  c->adj.off, c->adj.arg, c->adj.eph};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : c->events) {
@@ -1314,6 +1328,222 @@ int ladds_gpu_functor_pairs(ladds_gpu_ctx *c, const ladds_scan_params *p, size_t
   if (recs.size() > cap || (!out && !recs.empty()))
     return fail(c, LADDS_ERR_CAPACITY, "output buffer too small for the pair records");
   if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
+  return LADDS_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Adjoint of the propagation for conjunction pairs (kernels in adjoint.cuh).
+namespace {
+
+template <typename T>
+int ensureDev(ladds_gpu_ctx *c, T *&p, size_t &cap, size_t need) {
+  if (need <= cap && p) return LADDS_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    return fail(c, LADDS_ERR_ALLOC, "device allocation for the adjoint pair batch failed");
+  }
+  cap = need;
+  return LADDS_OK;
+}
+
+// buffers of nPairs pairs, `steps` steps, checkpoints every ck; ephemeris of the steps
+int adjPrepare(ladds_gpu_ctx *c, size_t nPairs, int steps, int ck, bool backward) {
+  auto &A = c->adj;
+  const size_t nObj = 2 * nPairs;
+  size_t objCap = A.objCap;
+  int rc;
+  if (nObj > A.objCap) {
+    size_t cap0 = 0, cap1 = 0, cap2 = 0, cap3 = 0, cap4 = 0, cap5 = 0, cap6 = 0;
+    if ((rc = ensureDev(c, A.st, cap0, 6 * nObj)) || (rc = ensureDev(c, A.bc, cap1, nObj)) ||
+        (rc = ensureDev(c, A.aom, cap2, nObj)) || (rc = ensureDev(c, A.miss, cap3, nPairs)) ||
+        (rc = ensureDev(c, A.grad, cap4, 7 * nObj)) || (rc = ensureDev(c, A.arg, cap5, nPairs)) ||
+        (rc = ensureDev(c, A.off, cap6, 6 * nPairs))) {
+      A.objCap = 0;
+      return rc;
+    }
+    objCap = nObj;
+  }
+  A.objCap = objCap;
+  const size_t nSeg = (size_t)((steps + ck - 1) / ck);
+  if ((rc = ensureDev(c, A.ckpt, A.ckptCap, nSeg * 6 * nObj))) return rc;
+  if (backward && (rc = ensureDev(c, A.rec, A.recCap, (size_t)ck * 15 * nObj))) return rc;
+  if ((rc = ensureDev(c, A.eph, A.ephCap, (size_t)3 * steps))) return rc;
+  return LADDS_OK;
+}
+
+int adjEphemeris(ladds_gpu_ctx *c, int steps) {
+  k_ephemeris<<<blocksFor((size_t)3 * steps, 128), 128, 0, c->st>>>(c->adj.eph, steps, 0, c->cfg.startTime,
+                                                                     c->cfg.deltaT, c->pc.hc1, c->pc.hc2,
+                                                                     c->cfg.epochJD, c->theta0);
+  CK(cudaGetLastError());
+  return LADDS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ladds_gpu_adjoint_forward(ladds_gpu_ctx *c, const ladds_adjoint_pair *pairs, size_t nPairs, int steps,
+                              int checkpointEvery, double *missSq, int32_t *tcaStep, double *loss,
+                              double *deviceMs) {
+  if (!c || (nPairs && !pairs) || steps < 1 || checkpointEvery < 1 || nPairs > (size_t)(1 << 29))
+    return fail(c, LADDS_ERR_INVALID_ARG, "adjoint_forward: bad argument");
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  CK(cudaSetDevice(c->dev));
+  auto &A = c->adj;
+  A.forwardDone = false;
+  int rc = adjPrepare(c, nPairs, steps, checkpointEvery, false);
+  if (rc) return rc;
+  const size_t nObj = 2 * nPairs;
+  // pairs (AoS) -> object SoA
+  std::vector<double> st(6 * nObj), bc(nObj), aom(nObj);
+  for (size_t p = 0; p < nPairs; ++p) {
+    const ladds_adjoint_pair &q = pairs[p];
+    for (int k = 0; k < 3; ++k) {
+      st[k * nObj + 2 * p] = q.rA[k];
+      st[(3 + k) * nObj + 2 * p] = q.vA[k];
+      st[k * nObj + 2 * p + 1] = q.rB[k];
+      st[(3 + k) * nObj + 2 * p + 1] = q.vB[k];
+    }
+    bc[2 * p] = q.bcInvA;
+    bc[2 * p + 1] = q.bcInvB;
+    aom[2 * p] = q.aomA;
+    aom[2 * p + 1] = q.aomB;
+  }
+  if (nObj) {
+    CK(cudaMemcpyAsync(A.st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(A.bc, bc.data(), bc.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(A.aom, aom.data(), aom.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  }
+  if ((rc = adjEphemeris(c, steps))) return rc;
+  CK(cudaEventRecord(c->callStart, c->st));
+  if (nObj)
+    k_adj_forward<<<blocksFor(nObj, 128), 128, 0, c->st>>>(A.st, A.bc, A.aom, (int)nObj, steps, checkpointEvery,
+                                                           A.eph, c->pc, c->cfg.deltaT, A.ckpt, A.miss, A.arg);
+  CK(cudaEventRecord(c->callEnd, c->st));
+  CK(cudaGetLastError());
+  std::vector<double> miss(nPairs);
+  std::vector<int> arg(nPairs);
+  if (nPairs) {
+    CK(cudaMemcpyAsync(miss.data(), A.miss, nPairs * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(arg.data(), A.arg, nPairs * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->callStart, c->callEnd));
+  if (deviceMs) *deviceMs = ms;
+  double sum = 0.0;
+  for (size_t p = 0; p < nPairs; ++p) {
+    if (missSq) missSq[p] = miss[p];
+    if (tcaStep) tcaStep[p] = arg[p];
+    if (arg[p] > 0) sum += miss[p];
+  }
+  if (loss) *loss = sum;
+  A.nPairs = nPairs;
+  A.steps = steps;
+  A.ck = checkpointEvery;
+  A.forwardDone = true;
+  return LADDS_OK;
+}
+
+int ladds_gpu_adjoint_backward(ladds_gpu_ctx *c, double *dL_dx0, double *dL_dbc, double *deviceMs) {
+  if (!c || !dL_dx0 || !dL_dbc) return fail(c, LADDS_ERR_INVALID_ARG, "adjoint_backward: null output");
+  auto &A = c->adj;
+  if (!A.forwardDone) return fail(c, LADDS_ERR_STATE, "adjoint_backward needs a preceding adjoint_forward");
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  CK(cudaSetDevice(c->dev));
+  int rc = adjPrepare(c, A.nPairs, A.steps, A.ck, true);
+  if (rc) return rc;
+  const size_t nObj = 2 * A.nPairs;
+  CK(cudaEventRecord(c->callStart, c->st));
+  if (nObj)
+    k_adj_backward<<<blocksFor(nObj, 128), 128, 0, c->st>>>(A.bc, A.aom, (int)nObj, A.steps, A.ck, A.eph, c->pc,
+                                                            c->cfg.deltaT, A.ckpt, A.arg, A.rec, A.grad);
+  CK(cudaEventRecord(c->callEnd, c->st));
+  CK(cudaGetLastError());
+  std::vector<double> g(7 * nObj);
+  if (nObj) CK(cudaMemcpyAsync(g.data(), A.grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->callStart, c->callEnd));
+  if (deviceMs) *deviceMs = ms;
+  for (size_t p = 0; p < A.nPairs; ++p) {
+    for (int k = 0; k < 6; ++k) {
+      dL_dx0[12 * p + k] = g[k * nObj + 2 * p];
+      dL_dx0[12 * p + 6 + k] = g[k * nObj + 2 * p + 1];
+    }
+    dL_dbc[2 * p] = g[6 * nObj + 2 * p];
+    dL_dbc[2 * p + 1] = g[6 * nObj + 2 * p + 1];
+  }
+  return LADDS_OK;
+}
+
+int ladds_gpu_adjoint_make_pairs(ladds_gpu_ctx *c, uint64_t seed, size_t nPairs, int steps,
+                                 ladds_adjoint_pair *out, int32_t *tcaStep) {
+  if (!c || (nPairs && !out) || steps < 2 || nPairs > (size_t)(1 << 29))
+    return fail(c, LADDS_ERR_INVALID_ARG, "adjoint_make_pairs: bad argument");
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  CK(cudaSetDevice(c->dev));
+  auto &A = c->adj;
+  A.forwardDone = false;
+  int rc = adjPrepare(c, nPairs, steps, steps, false);
+  if (rc) return rc;
+  const size_t nObj = 2 * nPairs;
+  std::vector<double> st(6 * nObj), bc(nObj), aom(nObj), off(6 * nPairs);
+  std::vector<int> tca(nPairs);
+  for (size_t p = 0; p < nPairs; ++p) {
+    double sa[6], sb[6], dr[3], dv[3];
+    adjointPairDraw(seed, p, c->cfg.deltaT, steps, sa, sb, bc[2 * p], aom[2 * p], bc[2 * p + 1], aom[2 * p + 1],
+                    dr, dv, tca[p]);
+    for (int k = 0; k < 6; ++k) {
+      st[k * nObj + 2 * p] = sa[k];
+      st[k * nObj + 2 * p + 1] = sb[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+      off[6 * p + k] = dr[k];
+      off[6 * p + 3 + k] = dv[k];
+    }
+  }
+  int *dTca = A.arg;  // the forward's argmin buffer serves as scratch here
+  if (nObj) {
+    CK(cudaMemcpyAsync(A.st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(A.bc, bc.data(), bc.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(A.aom, aom.data(), aom.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(A.off, off.data(), off.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dTca, tca.data(), tca.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+  }
+  if ((rc = adjEphemeris(c, steps))) return rc;
+  PropConsts back = c->pc;
+  back.hc1 = -back.hc1;
+  back.hc2 = -back.hc2;
+  back.hd1 = -back.hd1;
+  back.hd2 = -back.hd2;
+  if (nPairs)
+    k_adj_make_pairs<<<blocksFor(nPairs, 128), 128, 0, c->st>>>(A.st, A.bc, A.aom, (int)nPairs, dTca, A.off, A.eph,
+                                                                c->pc, back);
+  CK(cudaGetLastError());
+  if (nObj) CK(cudaMemcpyAsync(st.data(), A.st, st.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (size_t p = 0; p < nPairs; ++p) {
+    ladds_adjoint_pair &q = out[p];
+    for (int k = 0; k < 3; ++k) {
+      q.rA[k] = st[k * nObj + 2 * p];
+      q.vA[k] = st[(3 + k) * nObj + 2 * p];
+      q.rB[k] = st[k * nObj + 2 * p + 1];
+      q.vB[k] = st[(3 + k) * nObj + 2 * p + 1];
+    }
+    q.bcInvA = bc[2 * p];
+    q.bcInvB = bc[2 * p + 1];
+    q.aomA = aom[2 * p];
+    q.aomB = aom[2 * p + 1];
+    if (tcaStep) tcaStep[p] = tca[p];
+  }
   return LADDS_OK;
 }
 

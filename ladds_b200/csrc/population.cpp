@@ -16,6 +16,7 @@
 
 #include "../../include/ladds_gpu.h"
 #include "physics.cuh"
+#include "population.h"
 
 namespace {
 
@@ -80,8 +81,9 @@ void setObject(const Out &o, size_t k, const double r[3], const double v[3], dou
   o.act[k] = (int8_t)activity;
 }
 
-// population 0 element draw
-void background(const Out &o, uint64_t seed, size_t k) {
+// population 0 element draw of object k; el (may be null) receives a, e, i, RAAN, argp, M
+void drawBackground(uint64_t seed, size_t k, double r[3], double v[3], double &radius, double &mass,
+                    double *el = nullptr) {
   Rng g(seed, k);
   const double h = 400.0 + 1100.0 * g.uniform();
   const double e = 0.02 * g.uniform();
@@ -89,10 +91,22 @@ void background(const Out &o, uint64_t seed, size_t k) {
   const double raan = 2.0 * ladds::kPi * g.uniform();
   const double argp = 2.0 * ladds::kPi * g.uniform();
   const double M = 2.0 * ladds::kPi * g.uniform();
-  const double radius = std::exp(std::log(0.01) + (std::log(5.0) - std::log(0.01)) * g.uniform());
-  const double mass = kRho * (4.0 / 3.0) * ladds::kPi * radius * radius * radius;
-  double r[3], v[3];
+  radius = std::exp(std::log(0.01) + (std::log(5.0) - std::log(0.01)) * g.uniform());
+  mass = kRho * (4.0 / 3.0) * ladds::kPi * radius * radius * radius;
   ladds_elements_to_state(ladds::kREarth + h, e, inc, raan, argp, M, r, v);
+  if (el) {
+    el[0] = ladds::kREarth + h;
+    el[1] = e;
+    el[2] = inc;
+    el[3] = raan;
+    el[4] = argp;
+    el[5] = M;
+  }
+}
+
+void background(const Out &o, uint64_t seed, size_t k) {
+  double r[3], v[3], radius, mass;
+  drawBackground(seed, k, r, v, radius, mass);
   setObject(o, k, r, v, radius, mass, LADDS_PASSIVE);
 }
 
@@ -194,3 +208,59 @@ extern "C" int ladds_population_generate(int which, uint64_t seed, size_t n, dou
   }
   return LADDS_ERR_INVALID_ARG;
 }
+
+namespace ladds {
+
+namespace {
+// two-body perigee radius of (r, v); +inf-free: returns 0 for open orbits
+double perigeeRadius(const double r[3], const double v[3]) {
+  const double rn = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const double inv = 2.0 / rn - v2 / kMuEarth;
+  if (!(inv > 0.0)) return 0.0;
+  const double a = 1.0 / inv;
+  const double h[3] = {r[1] * v[2] - r[2] * v[1], r[2] * v[0] - r[0] * v[2], r[0] * v[1] - r[1] * v[0]};
+  const double ev[3] = {(v[1] * h[2] - v[2] * h[1]) / kMuEarth - r[0] / rn,
+                        (v[2] * h[0] - v[0] * h[2]) / kMuEarth - r[1] / rn,
+                        (v[0] * h[1] - v[1] * h[0]) / kMuEarth - r[2] / rn};
+  return a * (1.0 - std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]));
+}
+}  // namespace
+
+void adjointPairDraw(uint64_t seed, size_t p, double dt, int steps, double stA[6], double stB[6], double &bcA,
+                     double &aomA, double &bcB, double &aomB, double dr[3], double dv[3], int &tca) {
+  double radius, mass, el[6];
+  drawBackground(seed, 2 * p, stA, stA + 3, radius, mass, el);
+  double area = kPi * radius * radius;
+  aomA = area * 1e-6 / mass;
+  bcA = kCd * area / mass;
+  const double period = 2.0 * kPi * std::sqrt(el[0] * el[0] * el[0] / kMuEarth);
+  const long n = std::lround(1.5 * period / std::fabs(dt));
+  tca = (int)std::max(1L, std::min((long)steps - 1, n));
+  drawBackground(seed, 2 * p + 1, stB, stB + 3, radius, mass);
+  area = kPi * radius * radius;
+  aomB = area * 1e-6 / mass;
+  bcB = kCd * area / mass;
+  // A's two-body state at the close approach (mean motion only) for the perigee check of B
+  double rK[3], vK[3];
+  ladds_elements_to_state(el[0], el[1], el[2], el[3], el[4], el[5] + 2.0 * kPi * tca * std::fabs(dt) / period, rK,
+                          vK);
+  Rng g(seed ^ 0x5A17C0DE5A17C0DEull, p);
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    const double mr = 0.05 + 1.95 * g.uniform(), mv = 0.01 + 0.49 * g.uniform();
+    double u[3], w[3];
+    for (int k = 0; k < 3; ++k) u[k] = g.normal();
+    for (int k = 0; k < 3; ++k) w[k] = g.normal();
+    const double un = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double wn = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    for (int k = 0; k < 3; ++k) {
+      dr[k] = mr * u[k] / un;
+      dv[k] = mv * w[k] / wn;
+    }
+    const double rB[3] = {rK[0] + dr[0], rK[1] + dr[1], rK[2] + dr[2]};
+    const double vB[3] = {vK[0] + dv[0], vK[1] + dv[1], vK[2] + dv[2]};
+    if (perigeeRadius(rB, vB) >= kREarth + kPairMinPerigeeAltitude) break;  // else redraw
+  }
+}
+
+}  // namespace ladds

@@ -583,3 +583,242 @@ size_t oracle_step(size_t n, double *x, double *y, double *z, double *vx, double
   return oracle_scan_cells(n, x, y, z, vx, vy, vz, radius, id, parent, activity, dummy, p, g, step, out, cap,
                            nthreads);
 }
+
+/* ===================== differentiation checks =====================
+ * Tangent-linear (forward-mode) restatement of the pair loss used to check the
+ * adjoint: every quantity carries its derivative along one direction of the
+ * 14 inputs of a pair (rA, vA, rB, vB, bcInvA, bcInvB).  The reference has no
+ * differentiation; the primal below is oracle_propagate's step and
+ * oracle_interpolate (DistanceApproximation.cpp:13-58) with the same
+ * evaluation order. */
+typedef struct {
+  double v, d;
+} od;
+
+static inline od od_c(double v) {
+  od r = {v, 0.0};
+  return r;
+}
+static inline od od_add(od a, od b) {
+  od r = {a.v + b.v, a.d + b.d};
+  return r;
+}
+static inline od od_sub(od a, od b) {
+  od r = {a.v - b.v, a.d - b.d};
+  return r;
+}
+static inline od od_mul(od a, od b) {
+  od r = {a.v * b.v, a.d * b.v + a.v * b.d};
+  return r;
+}
+static inline od od_muls(od a, double s) {
+  od r = {a.v * s, a.d * s};
+  return r;
+}
+static inline od od_div(od a, od b) {
+  const double q = a.v / b.v;
+  od r = {q, (a.d - q * b.d) / b.v};
+  return r;
+}
+static inline od od_sqrt(od a) {
+  const double s = sqrt(a.v);
+  od r = {s, a.d / (2.0 * s)};
+  return r;
+}
+static inline od od_exp(od a) {
+  const double e = exp(a.v);
+  od r = {e, e * a.d};
+  return r;
+}
+static inline od od_dot3(const od a[3], const od b[3]) {
+  od r = od_c(0.0);
+  r = od_add(r, od_mul(a[0], b[0]));
+  r = od_add(r, od_mul(a[1], b[1]));
+  r = od_add(r, od_mul(a[2], b[2]));
+  return r;
+}
+
+/* oracle_accel in dual arithmetic (passive object) */
+static void accel_dual(uint32_t mask, const od r[3], const od v[3], double aom, od bcInv, const oracle_ephem *e,
+                       od a[3]) {
+  const od x = r[0], y = r[1], z = r[2];
+  const od r2 = od_add(od_add(od_mul(x, x), od_mul(y, y)), od_mul(z, z));
+  const od rn = od_sqrt(r2);
+  const od rinv = od_div(od_c(1.0), rn);
+  const od rinv2 = od_mul(rinv, rinv);
+  od ax = od_c(0.0), ay = od_c(0.0), az = od_c(0.0);
+  if (mask & OR_KEP) {
+    const od k = od_mul(od_muls(rinv2, -OR_MU_EARTH), rinv);
+    ax = od_add(ax, od_mul(k, x));
+    ay = od_add(ay, od_mul(k, y));
+    az = od_add(az, od_mul(k, z));
+  }
+  if (mask & OR_J2M) {
+    const double c = -1.5 * OR_J2 * OR_MU_EARTH * OR_R_EARTH * OR_R_EARTH;
+    const od k = od_mul(od_mul(od_muls(rinv2, c), rinv2), rinv);
+    const od zr2 = od_mul(od_mul(z, z), rinv2);
+    const od f1 = od_sub(od_c(1.0), od_muls(zr2, 5.0)), f3 = od_sub(od_c(3.0), od_muls(zr2, 5.0));
+    ax = od_add(ax, od_mul(od_mul(k, x), f1));
+    ay = od_add(ay, od_mul(od_mul(k, y), f1));
+    az = od_add(az, od_mul(od_mul(k, z), f3));
+  }
+  if (mask & OR_J3M) {
+    const double c = -2.5 * OR_J3 * OR_MU_EARTH * OR_R_EARTH * OR_R_EARTH * OR_R_EARTH;
+    const od k = od_mul(od_mul(od_mul(od_muls(rinv2, c), rinv2), rinv2), rinv);
+    const od z2 = od_mul(z, z);
+    const od f = od_sub(od_muls(z, 3.0), od_mul(od_mul(od_muls(z2, 7.0), z), rinv2));
+    ax = od_add(ax, od_mul(od_mul(k, x), f));
+    ay = od_add(ay, od_mul(od_mul(k, y), f));
+    const od fz = od_sub(od_sub(od_muls(z2, 6.0), od_mul(od_mul(od_muls(z2, 7.0), z2), rinv2)), od_muls(r2, 0.6));
+    az = od_add(az, od_mul(k, fz));
+  }
+  if (mask & (OR_C22 | OR_S22)) {
+    const double C = (mask & OR_C22) ? OR_C22_BAR * OR_N22 : 0.0;
+    const double S = (mask & OR_S22) ? OR_S22_BAR * OR_N22 : 0.0;
+    const double c = e->cosT, s = e->sinT;
+    const od xf = od_add(od_muls(x, c), od_muls(y, s)), yf = od_add(od_muls(x, -s), od_muls(y, c));
+    const od g = od_add(od_muls(od_sub(od_mul(xf, xf), od_mul(yf, yf)), C), od_mul(od_muls(xf, 2.0 * S), yf));
+    const double kc = 3.0 * OR_MU_EARTH * OR_R_EARTH * OR_R_EARTH;
+    const od k = od_mul(od_mul(od_muls(rinv2, kc), rinv2), rinv);
+    const od axf =
+        od_mul(k, od_sub(od_muls(od_add(od_muls(xf, C), od_muls(yf, S)), 2.0), od_mul(od_muls(g, 5.0), od_mul(xf, rinv2))));
+    const od ayf =
+        od_mul(k, od_sub(od_muls(od_sub(od_muls(xf, S), od_muls(yf, C)), 2.0), od_mul(od_muls(g, 5.0), od_mul(yf, rinv2))));
+    const od azf = od_mul(k, od_mul(od_muls(g, -5.0), od_mul(z, rinv2)));
+    ax = od_add(ax, od_sub(od_muls(axf, c), od_muls(ayf, s)));
+    ay = od_add(ay, od_add(od_muls(axf, s), od_muls(ayf, c)));
+    az = od_add(az, azf);
+  }
+  for (int body = 0; body < 2; ++body) {
+    const uint32_t bit = body == 0 ? OR_SOL : OR_LUN;
+    if (!(mask & bit)) continue;
+    const double *s = body == 0 ? e->sun : e->moon;
+    const double mu = body == 0 ? OR_MU_SUN : OR_MU_MOON;
+    const od dx = od_sub(od_c(s[0]), x), dy = od_sub(od_c(s[1]), y), dz = od_sub(od_c(s[2]), z);
+    const od d2 = od_add(od_add(od_mul(dx, dx), od_mul(dy, dy)), od_mul(dz, dz));
+    const od dn = od_sqrt(d2);
+    const double s2 = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    const double sn = sqrt(s2);
+    const od kd = od_div(od_c(mu), od_mul(d2, dn));
+    const double ks = mu / (s2 * sn);
+    ax = od_add(ax, od_sub(od_mul(kd, dx), od_c(ks * s[0])));
+    ay = od_add(ay, od_sub(od_mul(kd, dy), od_c(ks * s[1])));
+    az = od_add(az, od_sub(od_mul(kd, dz), od_c(ks * s[2])));
+  }
+  if (mask & OR_SRP) {
+    const double *s = e->sun;
+    const double s2 = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    const double proj = (x.v * s[0] + y.v * s[1] + z.v * s[2]) / sqrt(s2);
+    const int shadow = proj < 0.0 && (r2.v - proj * proj) < OR_R_EARTH * OR_R_EARTH;
+    if (!shadow) {
+      const od ux = od_sub(x, od_c(s[0])), uy = od_sub(y, od_c(s[1])), uz = od_sub(z, od_c(s[2]));
+      const od u2 = od_add(od_add(od_mul(ux, ux), od_mul(uy, uy)), od_mul(uz, uz));
+      const od un = od_sqrt(u2);
+      const od k = od_div(od_muls(od_div(od_c(OR_AU * OR_AU), u2), OR_C_R * OR_P_SRP * aom * 1.0e3), un);
+      ax = od_add(ax, od_mul(k, ux));
+      ay = od_add(ay, od_mul(k, uy));
+      az = od_add(az, od_mul(k, uz));
+    }
+  }
+  if (mask & OR_DRAG) {
+    const od wx = od_add(v[0], od_muls(y, OR_OMEGA_EARTH)), wy = od_sub(v[1], od_muls(x, OR_OMEGA_EARTH)),
+             wz = v[2];
+    const od wn = od_sqrt(od_add(od_add(od_mul(wx, wx), od_mul(wy, wy)), od_mul(wz, wz)));
+    const od h = od_sub(rn, od_c(OR_R_EARTH));
+    const int b = atm_band(h.v);
+    const od rho = od_muls(od_exp(od_muls(od_sub(h, od_c(OR_ATM[b][0])), -1.0 / OR_ATM[b][2])), OR_ATM[b][1]);
+    const od k = od_mul(od_muls(od_mul(rho, bcInv), -0.5 * 1.0e3), wn);
+    ax = od_add(ax, od_mul(k, wx));
+    ay = od_add(ay, od_mul(k, wy));
+    az = od_add(az, od_mul(k, wz));
+  }
+  a[0] = ax;
+  a[1] = ay;
+  a[2] = az;
+}
+
+/* oracle_interpolate in dual arithmetic; returns |dr|^2 */
+static od miss_dual(const od ri[3], const od vi[3], const od rj[3], const od vj[3], double dt) {
+  od oi[3], oj[3];
+  for (int k = 0; k < 3; ++k) {
+    oi[k] = od_sub(ri[k], od_muls(vi[k], dt));
+    oj[k] = od_sub(rj[k], od_muls(vj[k], dt));
+  }
+  const od vi_ri = od_dot3(vi, oi), vi_rj = od_dot3(vi, oj), vj_ri = od_dot3(vj, oi), vj_rj = od_dot3(vj, oj);
+  const od num = od_sub(od_sub(od_add(vi_rj, vj_ri), vi_ri), vj_rj);
+  const od two = od_muls(od_dot3(vi, vj), 2.0);
+  const od den = od_sub(od_add(od_dot3(vi, vi), od_dot3(vj, vj)), two);
+  od t = od_div(num, den);
+  if (t.v < 0.0)
+    t = od_c(0.0);
+  else if (dt < t.v)
+    t = od_c(dt);
+  od dr[3];
+  for (int k = 0; k < 3; ++k) {
+    const od p1 = od_add(oi[k], od_mul(vi[k], t));
+    const od p2 = od_add(oj[k], od_mul(vj[k], t));
+    dr[k] = od_sub(p1, p2);
+  }
+  return od_dot3(dr, dr);
+}
+
+void oracle_pair_losses(size_t nPairs, const double *pairs, const double *dirs, uint32_t mask, double jdEpoch,
+                        double t0, double dt, int steps, double *miss, int32_t *tca, double *dmiss, int nthreads) {
+  if (steps <= 0 || nPairs == 0) return;
+  const double theta0 = oracle_gmst0(jdEpoch);
+  oracle_ephem *eph = (oracle_ephem *)malloc((size_t)steps * 3 * sizeof(oracle_ephem));
+  const double hc1 = OR_YOSHIDA_C1 * dt, hc2 = OR_YOSHIDA_C2 * dt;
+  const double hd1 = OR_YOSHIDA_D1 * dt, hd2 = OR_YOSHIDA_D2 * dt;
+  for (int s = 0; s < steps; ++s) {
+    const double tn = t0 + (double)s * dt;
+    const double tau1 = tn + hc1, tau2 = tau1 + hc2, tau3 = tau2 + hc2;
+    oracle_ephemeris(jdEpoch, theta0, tau1, &eph[3 * s + 0]);
+    oracle_ephemeris(jdEpoch, theta0, tau2, &eph[3 * s + 1]);
+    oracle_ephemeris(jdEpoch, theta0, tau3, &eph[3 * s + 2]);
+  }
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (size_t p = 0; p < nPairs; ++p) {
+    const double *q = pairs + 16 * p;
+    const double *d = dirs ? dirs + 14 * p : NULL;
+    od r[2][3], v[2][3], bc[2];
+    double aom[2] = {q[14], q[15]};
+    for (int o = 0; o < 2; ++o) {
+      for (int k = 0; k < 3; ++k) {
+        r[o][k].v = q[6 * o + k];
+        r[o][k].d = d ? d[6 * o + k] : 0.0;
+        v[o][k].v = q[6 * o + 3 + k];
+        v[o][k].d = d ? d[6 * o + 3 + k] : 0.0;
+      }
+      bc[o].v = q[12 + o];
+      bc[o].d = d ? d[12 + o] : 0.0;
+    }
+    double best = INFINITY, bestD = 0.0;
+    int arg = 0;
+    const double hk[3] = {hd1, hd2, hd1};
+    const double hdft[4] = {hc1, hc2, hc2, hc1};
+    for (int s = 0; s < steps; ++s) {
+      for (int o = 0; o < 2; ++o) {
+        od a[3];
+        for (int st = 0; st < 3; ++st) {
+          for (int k = 0; k < 3; ++k) r[o][k] = od_add(r[o][k], od_muls(v[o][k], hdft[st]));
+          accel_dual(mask, r[o], v[o], aom[o], bc[o], &eph[3 * s + st], a);
+          for (int k = 0; k < 3; ++k) v[o][k] = od_add(v[o][k], od_muls(a[k], hk[st]));
+        }
+        for (int k = 0; k < 3; ++k) r[o][k] = od_add(r[o][k], od_muls(v[o][k], hdft[3]));
+      }
+      const od d2 = miss_dual(r[0], v[0], r[1], v[1], dt);
+      if (d2.v < best) {
+        best = d2.v;
+        bestD = d2.d;
+        arg = s + 1;
+      }
+    }
+    miss[p] = best;
+    if (tca) tca[p] = arg;
+    if (dmiss) dmiss[p] = bestD;
+  }
+  free(eph);
+}

@@ -162,6 +162,17 @@ void oracle_propagate(size_t n, double *x, double *y, double *z, double *vx, dou
                       uint32_t mask, double jdEpoch, double t0, double dt, int steps, int nthreads);
 double oracle_density(double hKm);
 
+/* --- differentiation checks ---
+ * Pair loss restated in tangent-linear (dual-number) arithmetic.  pairs: 16
+ * doubles per pair (rA, vA, rB, vB, bcInvA, bcInvB, aomA, aomB); passive
+ * objects propagated with oracle_propagate's Yoshida step from t0.  miss[p] =
+ * min over steps 1..steps of the squared interpolated miss distance
+ * (oracle_interpolate, i = A, j = B), tca[p] its step (0: none finite).
+ * dirs (14 per pair: drA, dvA, drB, dvB, dbcA, dbcB; may be NULL): dmiss[p] =
+ * the derivative of miss[p] along dirs (forward mode through every step). */
+void oracle_pair_losses(size_t nPairs, const double *pairs, const double *dirs, uint32_t mask, double jdEpoch,
+                        double t0, double dt, int steps, double *miss, int32_t *tca, double *dmiss, int nthreads);
+
 /* one simulation iteration: integrate, then scan with dt (reference loop order). */
 size_t oracle_step(size_t n, double *x, double *y, double *z, double *vx, double *vy, double *vz,
                    const double *aom, const double *bcInv, const double *radius, const uint64_t *id,

@@ -102,6 +102,8 @@ def lib():
         L.oracle_accel.argtypes = [C.c_uint32, C.c_int, dp, dp, C.c_double, C.c_double, C.POINTER(Ephem), dp]
         L.oracle_propagate.argtypes = [C.c_size_t] + [C.c_void_p] * 10 + [
             C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
+        L.oracle_pair_losses.argtypes = [C.c_size_t, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.oracle_density.restype = C.c_double
         L.oracle_density.argtypes = [C.c_double]
         _lib = L
@@ -231,3 +233,18 @@ def propagate(pop: Population, mask, dt, steps, t0=0.0, jd_epoch=JD_EPOCH_2022, 
     lib().oracle_propagate(pop.n, _ptr(pop.x), _ptr(pop.y), _ptr(pop.z), _ptr(pop.vx), _ptr(pop.vy), _ptr(pop.vz),
                            _ptr(pop.aom), _ptr(pop.bc_inv), _ptr(pop.activity), _ptr(pop.dummy), mask, jd_epoch,
                            t0, dt, steps, nthreads)
+
+
+def pair_losses(pairs, steps, dt=10.0, mask=FULL, dirs=None, t0=0.0, jd_epoch=JD_EPOCH_2022, nthreads=0):
+    """Per-pair min over steps of the squared interpolated miss distance, its
+    step, and (with dirs, 14 per pair) its tangent-linear derivative along dirs.
+    pairs: (P, 16) float64 = rA, vA, rB, vB, bcInvA, bcInvB, aomA, aomB."""
+    pairs = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1, 16)
+    n = len(pairs)
+    miss = np.zeros(n)
+    tca = np.zeros(n, dtype=np.int32)
+    dmiss = np.zeros(n) if dirs is not None else None
+    d = None if dirs is None else np.ascontiguousarray(dirs, dtype=np.float64).reshape(n, 14)
+    lib().oracle_pair_losses(n, _ptr(pairs), _ptr(d), mask, jd_epoch, t0, dt, steps, _ptr(miss), _ptr(tca),
+                             _ptr(dmiss), nthreads)
+    return miss, tca, dmiss
