@@ -166,27 +166,42 @@ __device__ __forceinline__ void warpSortRow(uint32_t s0, uint32_t L, uint32_t r,
   }
 }
 
-// cellOff[c] = number of the row's objects in cells < c, c = 0..nx, from the
-// sorted cell indices ix[0..L) (one binary search per cell)
+// Entries per row of the cell-offset table: nx + 1 rounded up to 8, so that
+// every row starts on a 16-byte boundary.
+__host__ __device__ __forceinline__ uint32_t cellOffPitch(uint32_t nx) { return (nx + 8u) & ~7u; }
+
+// t[c] = number of the row's objects in cells < c, c = 0..nx, from the sorted
+// cell indices ix[0..L).  Each thread owns blocks of 8 consecutive cells
+// (c0 = 8 * first, then + 8 * stride): one binary search for the block's first
+// cell, a forward walk for the other seven, one 16-byte store.  Entries past nx
+// (row padding) are written too and never read.
 template <typename IxAt>
-__device__ __forceinline__ void fillCellOffsets(uint16_t *__restrict__ cellOff, uint32_t nx, uint32_t L,
-                                                IxAt ixAt, uint32_t first, uint32_t stride) {
-  for (uint32_t cc = first; cc <= nx; cc += stride) {
+__device__ __forceinline__ void fillCellOffsets(uint16_t *__restrict__ t, uint32_t nx, uint32_t L, IxAt ixAt,
+                                                uint32_t first, uint32_t stride) {
+  for (uint32_t c0 = 8u * first; c0 <= nx; c0 += 8u * stride) {
     uint32_t lo = 0, hi = L;
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (ixAt(mid) < cc)
+      if (ixAt(mid) < c0)
         lo = mid + 1;
       else
         hi = mid;
     }
-    cellOff[cc] = (uint16_t)lo;
+    uint32_t v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t c = c0 + (uint32_t)q;
+      while (lo < L && ixAt(lo) < c) ++lo;
+      v[q] = lo;
+    }
+    *reinterpret_cast<uint4 *>(t + c0) =
+        make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
   }
 }
 
 // One warp per row of <= 256 objects; longer rows go to the list of
-// k_bucket_sort_large.  cellOff (row-major, nx + 1 entries per row; may be
-// null) receives the offset of every cell of the row inside the row.
+// k_bucket_sort_large.  cellOff (row-major, cellOffPitch(nx) entries per row;
+// may be null) receives the offset of every cell of the row inside the row.
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_small(
     const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
     const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
@@ -223,8 +238,100 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_small(
     }
     __syncwarp();
     if (cellOff)
-      fillCellOffsets(cellOff + (size_t)r * (nx + 1), nx, L, [&](uint32_t i) { return (uint32_t)sIx[i]; },
+      fillCellOffsets(cellOff + (size_t)r * cellOffPitch(nx), nx, L, [&](uint32_t i) { return (uint32_t)sIx[i]; },
                       (uint32_t)lane, 32u);
+    __syncwarp();
+  }
+}
+
+// Counting sort inside the rows (grids with nx <= kRowCountMaxNx): one warp per
+// row of <= 256 objects.  The warp histograms the row's cell indices in
+// shared memory; their exclusive scan is the row's cell-offset table (written
+// to cellOff as is) and places every object in its cell; objects sharing a
+// cell are ranked by slot.  Longer rows go to the list of k_bucket_sort_large.
+// Shared memory per warp: countWords u32 counters (nx + 1 rounded up to 32),
+// then 256 slots, 256 sources and 256 cell indices.
+constexpr int kRowCountMaxNx = 1023;
+constexpr int kRowSortThreads = 128;
+__host__ __device__ __forceinline__ uint32_t rowCountWords(uint32_t nx) { return (nx + 32u) & ~31u; }
+__host__ __device__ __forceinline__ size_t rowSortSmem(uint32_t nx) {
+  return (size_t)(kRowSortThreads / 32) * (rowCountWords(nx) * 4u + 256u * 10u);
+}
+
+__global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
+    const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
+    const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
+    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff) {
+  extern __shared__ uint32_t smemRows[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t H = rowCountWords(nx), per = H / 32u;
+  uint32_t *hist = smemRows + (size_t)warp * (H + 256u * 2u + 128u);
+  uint32_t *tSlot = hist + H, *tSrc = tSlot + 256;
+  uint16_t *tIx = reinterpret_cast<uint16_t *>(tSrc + 256);
+  const uint32_t pitch = cellOffPitch(nx);
+  const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t r = warpId; r < nRows; r += nWarps) {
+    const uint32_t s0 = rowStart[r], L = rowStart[r + 1] - s0;
+    if (L == 0) continue;
+    if (L > 256u) {
+      if (lane == 0) longRows[atomicAdd(longCount, 1u)] = r;
+      continue;
+    }
+    for (uint32_t c = lane; c < H; c += 32) hist[c] = 0u;
+    __syncwarp();
+    uint32_t eIx[8], eSlot[8], eSrc[8], eArr[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t e = (uint32_t)(q * 32 + lane);
+      if (e < L) {
+        const unsigned long long v = rec[s0 + e];
+        eIx[q] = (uint32_t)(v >> 32);
+        eSlot[q] = (uint32_t)v;
+        eSrc[q] = src[s0 + e];
+        eArr[q] = atomicAdd(&hist[eIx[q]], 1u);
+      }
+    }
+    __syncwarp();
+    // exclusive scan of the counts: lane l owns counters [l * per, (l + 1) * per)
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < per; ++i) sum += hist[lane * per + i];
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    uint32_t run = incl - sum;
+    for (uint32_t i = 0; i < per; ++i) {
+      const uint32_t c = hist[lane * per + i];
+      hist[lane * per + i] = run;
+      run += c;
+    }
+    __syncwarp();
+    if (cellOff) {
+      uint16_t *t = cellOff + (size_t)r * pitch;
+      for (uint32_t c = lane; c <= nx; c += 32) t[c] = (uint16_t)hist[c];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t e = (uint32_t)(q * 32 + lane);
+      if (e < L) {
+        const uint32_t p = hist[eIx[q]] + eArr[q];
+        tSlot[p] = eSlot[q];
+        tSrc[p] = eSrc[q];
+        tIx[p] = (uint16_t)eIx[q];
+      }
+    }
+    __syncwarp();
+    for (uint32_t p = lane; p < L; p += 32) {
+      const uint32_t ix = tIx[p], c0 = hist[ix], c1 = hist[ix + 1], sl = tSlot[p];
+      uint32_t rank = 0;
+      for (uint32_t q = c0; q < c1; ++q) rank += tSlot[q] < sl ? 1u : 0u;
+      const uint32_t out = s0 + c0 + rank;
+      sortedKeys[out] = r * nx + ix;
+      perm[out] = tSrc[p];
+    }
     __syncwarp();
   }
 }
@@ -277,8 +384,8 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
       perm[s + i] = I[i];
     }
     if (cellOff && L <= 65535u)  // offsets are 16-bit; longer rows are searched by the scan
-      fillCellOffsets(cellOff + (size_t)r * (nx + 1), nx, L, [&](uint32_t i) { return (uint32_t)(V[i] >> 32); },
-                      threadIdx.x, blockDim.x);
+      fillCellOffsets(cellOff + (size_t)r * cellOffPitch(nx), nx, L,
+                      [&](uint32_t i) { return (uint32_t)(V[i] >> 32); }, threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }

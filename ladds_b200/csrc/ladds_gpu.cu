@@ -79,7 +79,7 @@ struct ladds_gpu_ctx {
   unsigned long long *sortRec = nullptr;  // (ix << 32 | slot) sort records of the bucket sort
   uint32_t *rowCounts = nullptr;          // objects per row, then the scatter cursors (2 x (nRows+1))
   uint32_t *longRows = nullptr, *longCount = nullptr;  // rows with more than 256 objects
-  uint16_t *cellOff = nullptr;            // per row: offset of every cell inside the row (nx + 1 entries)
+  uint16_t *cellOff = nullptr;            // per row: offset of every cell inside the row (cellOffPitch entries)
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
   float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
   double4 *vel4 = nullptr;                // vx, vy, vz, id of the cell order
@@ -454,9 +454,15 @@ void enqueueSort(ladds_gpu_ctx *c) {
         c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
   }
   PhaseScope ps(c, kPhRowsort, c->st, 2);
-  const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
-  k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
-      c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
+  if (nx <= (uint32_t)kRowCountMaxNx) {  // counting sort inside the rows
+    const int rowBlocks = std::min(blocksFor((size_t)nRows * 32, kRowSortThreads), 32 * c->evalBlocks);
+    k_bucket_sort_rows<<<rowBlocks, kRowSortThreads, rowSortSmem(nx), c->st>>>(
+        c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
+  } else {
+    const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
+    k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
+        c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
+  }
   k_bucket_sort_large<<<c->evalBlocks / 2, kBucketThreads, kLargeRow * 12, c->st>>>(
       c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   c->sortedKeys = c->keys1;
@@ -465,6 +471,9 @@ void enqueueSort(ladds_gpu_ctx *c) {
 
 inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf}; }
 
+// gathers the state into cell order (so that the next propagation, key pass and
+// gather read nearly sequentially: objects move about one cell per step) and
+// writes the packed scan copies
 void enqueueCells(ladds_gpu_ctx *c) {
   PhaseScope ps(c, kPhPermute, c->st);
   k_permute<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur, c->alt, c->perm, (int)c->n, scanPack(c),
@@ -740,7 +749,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   // cell-offset table of the rows: used when it fits 1 GiB (250^3 cells: 31 MB)
-  const size_t cellOffBytes = (size_t)c->nRows * ((size_t)c->grid.n[0] + 1) * sizeof(uint16_t);
+  const size_t cellOffBytes = (size_t)c->nRows * cellOffPitch((uint32_t)c->grid.n[0]) * sizeof(uint16_t);
   if (cellOffBytes <= ((size_t)1 << 30) && cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess) {
     cudaGetLastError();
     c->cellOff = nullptr;  // the scan then searches the sorted keys

@@ -49,7 +49,7 @@ __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xh
     return;
   }
   if (cellOff && rs1 - rs0 <= 65535u) {
-    const uint16_t *t = cellOff + (size_t)r2 * (nx + 1);
+    const uint16_t *t = cellOff + (size_t)r2 * cellOffPitch(nx);
     lo = rs0 + __ldg(&t[xlo]);
     hi = rs0 + __ldg(&t[xhi + 1]);
   } else {
@@ -59,8 +59,75 @@ __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xh
   }
 }
 
+// Binary32 pre-filter and exact binary64 gate of one candidate pair (j, k)
+// with its positions already loaded; survivors go to the warp's buffer.
+__device__ __forceinline__ void testCandidate(uint32_t j, uint32_t k, float4 mf, float4 q,
+                                              const double4 *__restrict__ pos4, double cutoffSq, double nearRel,
+                                              float cutF, uint2 *sCandW, uint32_t *sNW, uint2 *__restrict__ cand,
+                                              unsigned long long *__restrict__ candCount,
+                                              unsigned long long candCap) {
+  const float dx = mf.x - q.x, dy = mf.y - q.y, dz = mf.z - q.z;
+  const float lim = cutF + 2.0f * (mf.w + q.w);
+  if (dx * dx + dy * dy + dz * dz > lim * lim * 1.000001f) return;
+  const double4 me = pos4[j], o = pos4[k];
+  double d[3];
+  d[0] = __dsub_rn(me.x, o.x);
+  d[1] = __dsub_rn(me.y, o.y);
+  d[2] = __dsub_rn(me.z, o.z);
+  const double d2 = dot3rn(d, d);
+  if (d2 > cutoffSq && !nearBand(d2, cutoffSq, nearRel)) return;
+  const uint32_t slot = atomicAdd(sNW, 1u);  // shared counter: no global contention
+  if (slot < (uint32_t)kWarpCand)
+    sCandW[slot] = make_uint2(j, k);
+  else
+    appendCandidateGlobal(j, k, cand, candCount, candCap);
+}
+
+// owner lane of item t: the largest lane whose excl <= t (lanes with empty
+// windows share the next lane's excl, so the largest is the one that owns t)
+__device__ __forceinline__ int windowOwner(uint32_t excl, uint32_t item) {
+  int owner = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const uint32_t e = __shfl_sync(0xffffffffu, excl, owner + step);
+    if (e <= item) owner += step;
+  }
+  return owner;
+}
+
+// Warp-balanced walk of one neighbour row: lane l owns the window [lo, hi) of
+// its object; the windows of the warp are concatenated (exclusive prefix
+// `excl`) and dealt out 32 items per round, so every lane tests one pair per
+// round however uneven the windows are.
+__device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int lane, int warpBase,
+                                                const double4 *__restrict__ pos4, const float4 *__restrict__ posf,
+                                                double cutoffSq, double nearRel, float cutF, uint2 *sCandW,
+                                                uint32_t *sNW, uint2 *__restrict__ cand,
+                                                unsigned long long *__restrict__ candCount,
+                                                unsigned long long candCap) {
+  const uint32_t cnt = hi - lo;
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  const uint32_t excl = incl - cnt;
+  for (uint32_t base = 0; base < total; base += 32u) {
+    const uint32_t item = base + (uint32_t)lane;
+    const int owner = windowOwner(excl, item);
+    const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
+    if (item >= total) continue;
+    const uint32_t jj = (uint32_t)(warpBase + owner), k = oLo + (item - oEx);
+    testCandidate(jj, k, __ldg(&posf[jj]), __ldg(&posf[k]), pos4, cutoffSq, nearRel, cutF, sCandW, sNW, cand,
+                  candCount, candCap);
+  }
+}
+
 // cutF: cutoff * (1 + nearRel) rounded up, so that every pair the exact gate or
-// its near band accepts passes the binary32 test.
+// its near band accepts passes the binary32 test.  The loops over the
+// neighbour rows are warp-uniform; inactive lanes contribute empty windows.
 __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__restrict__ tags,
                                                               const double4 *__restrict__ pos4,
                                                               const float4 *__restrict__ posf, int n,
@@ -76,53 +143,38 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) sN[warp] = 0;
   __syncwarp();
-  const int j = blockIdx.x * kScanCta + (int)threadIdx.x;
+  const int warpBase = blockIdx.x * kScanCta + warp * 32;
+  const int j = warpBase + lane;
   const bool inRange = j < n;
   const uint32_t myTag = inRange ? tags[j] : kTagDummy;
   const bool active = inRange && !tagDummy(myTag);
+  const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
+  int32_t ix = 0, iy = 0, iz = 0;
   if (active) {
-    const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
     const uint32_t key = skeys[j];
-    const double4 me = pos4[j];
-    const float4 mf = posf[j];
-    const int32_t ix = (int32_t)(key % (uint32_t)nx);
+    ix = (int32_t)(key % (uint32_t)nx);
     const uint32_t row = key / (uint32_t)nx;
-    const int32_t iy = (int32_t)(row % (uint32_t)ny), iz = (int32_t)(row / (uint32_t)ny);
-    const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
-    for (int dz = 0; dz <= R; ++dz) {
-      const int32_t jz = iz + dz;
-      if (jz >= nz) break;
-      for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
-        const int32_t jy = iy + dy;
-        if (jy < 0 || jy >= ny) continue;
+    iy = (int32_t)(row % (uint32_t)ny);
+    iz = (int32_t)(row / (uint32_t)ny);
+  }
+  const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
+  for (int dz = 0; dz <= R; ++dz) {
+    for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
+      const int32_t jz = iz + dz, jy = iy + dy;
+      uint32_t lo = 0, hi = 0;
+      if (active && jz < nz && jy >= 0 && jy < ny) {
         const uint32_t r2 = (uint32_t)jz * (uint32_t)ny + (uint32_t)jy;
-        uint32_t lo, hi;
         if (dz == 0 && dy == 0) {
           uint32_t l0;
           rowWindow(r2, (uint32_t)ix, xhi, (uint32_t)nx, rowStart, cellOff, skeys, l0, hi);
           lo = (uint32_t)j + 1u;  // own cell: later objects only
+          if (hi < lo) hi = lo;
         } else {
           rowWindow(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo, hi);
         }
-        for (uint32_t k = lo; k < hi; ++k) {
-          const float4 q = __ldg(&posf[k]);
-          const float dx = mf.x - q.x, dy2 = mf.y - q.y, dz2 = mf.z - q.z;
-          const float lim = cutF + 2.0f * (mf.w + q.w);
-          if (dx * dx + dy2 * dy2 + dz2 * dz2 > lim * lim * 1.000001f) continue;
-          const double4 o = pos4[k];
-          double d[3];
-          d[0] = __dsub_rn(me.x, o.x);
-          d[1] = __dsub_rn(me.y, o.y);
-          d[2] = __dsub_rn(me.z, o.z);
-          const double d2 = dot3rn(d, d);
-          if (d2 > cutoffSq && !nearBand(d2, cutoffSq, nearRel)) continue;
-          const uint32_t slot = atomicAdd(&sN[warp], 1u);  // shared counter: no global contention
-          if (slot < (uint32_t)kWarpCand)
-            sCand[warp][slot] = make_uint2((uint32_t)j, k);
-          else
-            appendCandidateGlobal((uint32_t)j, k, cand, candCount, candCap);
-        }
       }
+      warpWindowPairs(lo, hi, lane, warpBase, pos4, posf, cutoffSq, nearRel, cutF, sCand[warp], &sN[warp], cand,
+                      candCount, candCap);
     }
   }
   // one global append per warp for its buffered candidates

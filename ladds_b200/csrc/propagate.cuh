@@ -42,7 +42,7 @@ __device__ __forceinline__ uint32_t cellKey(double x, double y, double z, const 
 }
 
 template <bool SPLIT, bool KEYS>
-__global__ void __launch_bounds__(256) k_propagate(DevState s, int n, int nSteps, int ephBase, PropConsts pc,
+__global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSteps, int ephBase, PropConsts pc,
                                                    GridDesc g, uint32_t *__restrict__ keys,
                                                    unsigned *__restrict__ status) {
   __shared__ AtmShared atm;
