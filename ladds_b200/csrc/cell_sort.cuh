@@ -6,13 +6,16 @@
 // (cell key, slot): identical to a stable sort by key of the population in
 // slot order, and independent of the order the arrays are in before the call.
 //
-//   1. k_bucket_count: objects per cell row (row = key / nx; warp-aggregated
-//      atomics), then an exclusive scan of the counts = the row-start table
-//      that the pair scan uses.
-//   2. k_bucket_scatter: each object to its row bucket (warp-aggregated cursor
-//      atomics), with its sort record (ix << 32 | slot) and source index.
-//   3. k_bucket_sort_small: one warp per row of <= 32 objects, bitonic sort of
-//      the records in registers; longer rows are listed for
+//   1. countRowArrival (inside the kernel that computes the keys): objects per
+//      cell row (row = key / nx; warp-aggregated atomics) and each object's
+//      arrival index inside its row; the exclusive scan of the counts is the
+//      row-start table that the pair scan uses.
+//   2. k_bucket_place: each object to its row bucket at rowStart + arrival,
+//      with its sort record (ix << 32 | slot) and source index.
+//   3. k_bucket_sort_rows (nx <= kRowCountMaxNx): one warp per row of <= 256
+//      objects, counting sort by cell index in shared memory, ties by slot;
+//      k_bucket_sort_small otherwise: warp bitonic sort of the records in
+//      registers.  Longer rows are listed for
 //   4. k_bucket_sort_large: one CTA per listed row, bitonic sort in shared
 //      memory (<= kLargeRow objects) or in global memory beyond that.
 // The bitonic network is the variant whose comparators all put the minimum at
@@ -34,36 +37,39 @@ __device__ __forceinline__ uint32_t laneMaskLt() {
   return m;
 }
 
-__global__ void __launch_bounds__(kBucketThreads) k_bucket_count(const uint32_t *__restrict__ keys, int n,
-                                                                 uint32_t nx, uint32_t *__restrict__ rowCount) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = j < n;
-  const uint32_t row = valid ? keys[j] / nx : 0xffffffffu;
-  const uint32_t peers = __match_any_sync(0xffffffffu, row);
-  if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&rowCount[row], (uint32_t)__popc(peers));
-}
-
-__global__ void __launch_bounds__(kBucketThreads) k_bucket_scatter(const uint32_t *__restrict__ keys,
-                                                                   const uint32_t *__restrict__ tags, int n,
-                                                                   uint32_t nx, const uint32_t *__restrict__ rowStart,
-                                                                   uint32_t *__restrict__ rowCursor,
-                                                                   unsigned long long *__restrict__ rec,
-                                                                   uint32_t *__restrict__ src) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+// Row count of a key inside the producing kernel: warp-aggregated atomicAdd on
+// rowCount[key / nx]; returns the object's arrival index inside its row (its
+// place among the row's objects in the scatter).  Every lane of the warp must
+// call it (valid = false for lanes without an object).
+__device__ __forceinline__ uint32_t countRowArrival(uint32_t key, bool valid, uint32_t nx,
+                                                   uint32_t *__restrict__ rowCount) {
   const int lane = threadIdx.x & 31;
-  const bool valid = j < n;
-  const uint32_t key = valid ? keys[j] : 0u;
   const uint32_t row = valid ? key / nx : 0xffffffffu;
   const uint32_t peers = __match_any_sync(0xffffffffu, row);
   const int leader = __ffs(peers) - 1;
   uint32_t base = 0;
-  if (valid && lane == leader) base = atomicAdd(&rowCursor[row], (uint32_t)__popc(peers));
+  if (valid && lane == leader) base = atomicAdd(&rowCount[row], (uint32_t)__popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (!valid) return;
-  const uint32_t pos = rowStart[row] + base + (uint32_t)__popc(peers & laneMaskLt());
-  if (pos >= (uint32_t)n) return;  // only reachable with inconsistent counts
-  const uint32_t ix = key - row * nx;
-  rec[pos] = ((unsigned long long)ix << 32) | tagSlot(tags[j]);
+  return base + (uint32_t)__popc(peers & laneMaskLt());
+}
+
+// Scatter with the arrival indices of countRowArrival: no atomics.
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_place(const uint32_t *__restrict__ keys,
+                                                                 const uint32_t *__restrict__ arrival,
+                                                                 const uint32_t *__restrict__ tags, int n,
+                                                                 uint32_t nx, const uint32_t *__restrict__ rowStart,
+                                                                 unsigned long long *__restrict__ rec,
+                                                                 uint32_t *__restrict__ src,
+                                                                 unsigned *__restrict__ status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t key = keys[j], row = key / nx;
+  const uint32_t pos = rowStart[row] + arrival[j];
+  if (pos >= rowStart[row + 1]) {  // only reachable with inconsistent counts
+    atomicOr(status, 4u);
+    return;
+  }
+  rec[pos] = ((unsigned long long)(key - row * nx) << 32) | tagSlot(tags[j]);
   src[pos] = (uint32_t)j;
 }
 

@@ -77,7 +77,7 @@ struct ladds_gpu_ctx {
   uint32_t *keys0 = nullptr, *keys1 = nullptr, *vals0 = nullptr, *vals1 = nullptr;
   uint32_t *sortedKeys = nullptr, *perm = nullptr;  // results of the last sort
   unsigned long long *sortRec = nullptr;  // (ix << 32 | slot) sort records of the bucket sort
-  uint32_t *rowCounts = nullptr;          // objects per row, then the scatter cursors (2 x (nRows+1))
+  uint32_t *rowCounts = nullptr;          // objects per row (nRows + 1 used of 2 x (nRows + 1))
   uint32_t *longRows = nullptr, *longCount = nullptr;  // rows with more than 256 objects
   uint16_t *cellOff = nullptr;            // per row: offset of every cell inside the row (cellOffPitch entries)
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
@@ -393,22 +393,28 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
     k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
     return;
   }
+  // with keys: the row counts of the coming sort are accumulated by the kernel
+  if (keys) cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st);
   PhaseScope ps(c, kPhProp, c->st, 2);  // propagation + iteration counter
   const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
   const int g = blocksFor(c->n, b);
   const int n = (int)c->n;
   const bool split = c->cfg.precision == LADDS_PRECISION_SPLIT;
+  uint32_t *rc = c->rowCounts, *arr = c->scratchC;
   if (split) {
     if (keys)
-      k_propagate<true, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<true, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, rc, arr,
+                                                  c->dStatus);
     else
-      k_propagate<true, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<true, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr,
+                                                   nullptr, c->dStatus);
   } else {
     if (keys)
-      k_propagate<false, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, c->dStatus);
+      k_propagate<false, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, rc, arr,
+                                                   c->dStatus);
     else
-      k_propagate<false, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0,
-                                                     c->dStatus);
+      k_propagate<false, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr,
+                                                    nullptr, c->dStatus);
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
 }
@@ -438,20 +444,19 @@ void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, ui
   k_scan_add<<<nb1, kScanBlock, 0, c->st>>>(out, (int)count, s1x);
 }
 
-// keys0 holds the keys of c->cur in current order -> sortedKeys (keys1), perm
-// (vals1) and the row-start table; order = sort by (cell key, slot)
+// keys0 holds the keys of c->cur in current order, rowCounts their row counts
+// and scratchC their arrival indices (k_propagate<*, true> or k_cell_keys) ->
+// sortedKeys (keys1), perm (vals1) and the row-start table; order = sort by
+// (cell key, slot)
 void enqueueSort(ladds_gpu_ctx *c) {
   const int n = (int)c->n;
   const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
-  uint32_t *rowCount = c->rowCounts, *rowCursor = c->rowCounts + nRows + 1;
   {
-    PhaseScope ps(c, kPhBucket, c->st, 2 + exclusiveScanKernels((size_t)nRows + 1));
-    cudaMemsetAsync(c->rowCounts, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), c->st);
+    PhaseScope ps(c, kPhBucket, c->st, 1 + exclusiveScanKernels((size_t)nRows + 1));
     cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
-    k_bucket_count<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(c->keys0, n, nx, rowCount);
-    enqueueExclusiveScan(c, rowCount, (size_t)nRows + 1, c->rowStart);
-    k_bucket_scatter<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
-        c->keys0, c->cur.tag, n, nx, c->rowStart, rowCursor, c->sortRec, c->vals0);
+    enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
+    k_bucket_place<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
+        c->keys0, c->scratchC, c->cur.tag, n, nx, c->rowStart, c->sortRec, c->vals0, c->dStatus);
   }
   PhaseScope ps(c, kPhRowsort, c->st, 2);
   if (nx <= (uint32_t)kRowCountMaxNx) {  // counting sort inside the rows
@@ -983,8 +988,9 @@ int scanState(ladds_gpu_ctx *c, const ScanConsts &sc, float cutF, std::vector<la
   for (int attempt = 0; attempt < 5; ++attempt) {
     CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
     CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
+    CK(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
     k_cell_keys<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, (int)c->n, c->grid,
-                                                          c->keys0);
+                                                          c->keys0, c->rowCounts, c->scratchC);
     enqueueSort(c);
     enqueueCells(c);
     enqueueScanWith(c, c->st, sc, cutF, c->dIter, -1);  // records carry the index of the last integrated iteration

@@ -12,6 +12,7 @@
 // (uniform across the warp).  The atmosphere table is staged in shared memory
 // (the band index diverges across the warp).
 #pragma once
+#include "cell_sort.cuh"
 #include "forces.cuh"
 #include "state.cuh"
 
@@ -41,9 +42,12 @@ __device__ __forceinline__ uint32_t cellKey(double x, double y, double z, const 
   return (iz * (uint32_t)g.n[1] + iy) * (uint32_t)g.n[0] + ix;
 }
 
+// KEYS: also writes the cell key of the end position and counts it into its
+// cell row (rowCount, arrival: see countRowArrival).
 template <bool SPLIT, bool KEYS>
 __global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSteps, int ephBase, PropConsts pc,
                                                    GridDesc g, uint32_t *__restrict__ keys,
+                                                   uint32_t *__restrict__ rowCount, uint32_t *__restrict__ arrival,
                                                    unsigned *__restrict__ status) {
   __shared__ AtmShared atm;
   for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
@@ -53,9 +57,15 @@ __global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSt
   }
   __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const uint32_t tag = s.tag[j];
-  double r[3] = {s.x[j], s.y[j], s.z[j]};
+  if (!KEYS && j >= n) return;
+  const bool inRange = j < n;
+  const uint32_t tag = inRange ? s.tag[j] : kTagDummy;
+  double r[3] = {0.0, 0.0, 0.0};
+  if (inRange) {
+    r[0] = s.x[j];
+    r[1] = s.y[j];
+    r[2] = s.z[j];
+  }
   if (!tagDummy(tag)) {
     double v[3] = {s.vx[j], s.vy[j], s.vz[j]};
     const double aom = s.aom[j], bc = s.bc[j];
@@ -92,7 +102,14 @@ __global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSt
     s.vy[j] = v[1];
     s.vz[j] = v[2];
   }
-  if (KEYS) keys[j] = cellKey(r[0], r[1], r[2], g);
+  if (KEYS) {  // every lane of the warp reaches this point
+    const uint32_t key = cellKey(r[0], r[1], r[2], g);
+    const uint32_t a = countRowArrival(key, inRange, (uint32_t)g.n[0], rowCount);
+    if (inRange) {
+      keys[j] = key;
+      arrival[j] = a;
+    }
+  }
 }
 
 // Ephemeris of the stage times of `nSteps` steps starting at iteration `iter`
@@ -110,10 +127,18 @@ __global__ void k_ephemeris(EphEntry *__restrict__ out, int nSteps, int64_t iter
   ephemeris(jdEpoch, theta0, tau, out[i]);
 }
 
+// cell keys of the current positions + their row counts (as k_propagate<*, true>)
 __global__ void k_cell_keys(const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
-                            int n, GridDesc g, uint32_t *__restrict__ keys) {
+                            int n, GridDesc g, uint32_t *__restrict__ keys, uint32_t *__restrict__ rowCount,
+                            uint32_t *__restrict__ arrival) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) keys[j] = cellKey(x[j], y[j], z[j], g);
+  const bool inRange = j < n;
+  const uint32_t key = inRange ? cellKey(x[j], y[j], z[j], g) : 0u;
+  const uint32_t a = countRowArrival(key, inRange, (uint32_t)g.n[0], rowCount);
+  if (inRange) {
+    keys[j] = key;
+    arrival[j] = a;
+  }
 }
 
 }  // namespace ladds
