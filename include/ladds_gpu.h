@@ -283,6 +283,27 @@ typedef struct {
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
 
+/* ---- autotuner ----
+ * No counterpart in the reference (its AutoPas container tunes its own
+ * traversal).  Times trials of the context's step on a copy of its population
+ * (each trial: a fresh context, a warm-up call, then stepsPerTrial timed
+ * iterations from the same start state) and applies the fastest to ctx:
+ *   1. cell edge: the current one, cutoff / R for reach R = 1..4 and 1.5 and 2
+ *      cutoffs, those within [20, 160] km;
+ *   2. propagateBlock x scanBlock in {128, 256}^2;
+ *   3. iterations per captured chunk (graph) in {32, 64, 128}.
+ * Results never depend on these (the scan is exact for any cell edge, records
+ * are sorted), only the speed does.  The context's state and iteration are
+ * unchanged.  trials (may be NULL with cap 0) receive every trial. */
+typedef struct {
+  double cellSize;          /* cell edge used [km] */
+  int32_t reach;            /* neighbour reach in cells */
+  int32_t propagateBlock, scanBlock, chunkSteps;
+  double msPerStep;         /* device time per iteration of the trial */
+} ladds_tune_trial;
+int ladds_gpu_autotune(ladds_gpu_ctx *ctx, int stepsPerTrial, ladds_tune_trial *trials, size_t cap, size_t *nTrials,
+                       ladds_tune_trial *best);
+
 /* ---- adjoint of the propagation for conjunction pairs ----
  * Loss of a batch of pairs (A_p, B_p) propagated independently from the
  * context's startTime with its deltaT and component mask, FP64:

@@ -83,7 +83,7 @@ EXPORTED = [
     "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
-    "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs",
+    "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune",
 ]
 
 ADJ_PAIR_DTYPE = np.dtype([("rA", "<f8", (3,)), ("vA", "<f8", (3,)), ("rB", "<f8", (3,)), ("vB", "<f8", (3,)),
@@ -93,6 +93,14 @@ assert ADJ_PAIR_DTYPE.itemsize == 128
 OBJECT_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("id", "<u8"),
                          ("parentId", "<u8"), ("activity", "<i4"), ("slot", "<u4")])
 assert OBJECT_DTYPE.itemsize == 80
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("cellSize", C.c_double), ("reach", C.c_int32), ("propagateBlock", C.c_int32),
+                ("scanBlock", C.c_int32), ("chunkSteps", C.c_int32), ("msPerStep", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ScanParams(C.Structure):
@@ -144,6 +152,7 @@ def lib():
     L.ladds_gpu_adjoint_forward.argtypes = [vp, vp, sz, i, i, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_backward.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_make_pairs.argtypes = [vp, C.c_uint64, sz, i, vp, vp]
+    L.ladds_gpu_autotune.argtypes = [vp, i, C.POINTER(TuneTrial), sz, C.POINTER(sz), C.POINTER(TuneTrial)]
     L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
     return L
@@ -385,6 +394,15 @@ class Context:
                 continue
             self._check(rc)
             return out[: n.value].copy()
+
+    def autotune(self, steps_per_trial: int = 16):
+        """Times cell edges, block shapes and chunk lengths; applies the fastest.
+        Returns (best, [trials]) as dicts."""
+        trials = (TuneTrial * 64)()
+        n = C.c_size_t()
+        best = TuneTrial()
+        self._check(self._L.ladds_gpu_autotune(self._h, steps_per_trial, trials, 64, C.byref(n), C.byref(best)))
+        return best.as_dict(), [trials[i].as_dict() for i in range(min(n.value, 64))]
 
     # ---- adjoint of the propagation for conjunction pairs
     def adjoint_make_pairs(self, seed: int, n_pairs: int, steps: int):

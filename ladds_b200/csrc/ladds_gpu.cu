@@ -112,6 +112,7 @@ struct ladds_gpu_ctx {
   size_t objCap = 0;
   int evalBlocks = 592;     // grid of the candidate-evaluation kernel (4 per SM)
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
+  int chunkSteps = kMaxEphSteps;  // iterations per ephemeris chunk / captured graph (autotuned)
   struct Adjoint {          // buffers of the adjoint pair batch (ladds_gpu_adjoint_*)
     size_t nPairs = 0;
     int steps = 0, ck = 0;
@@ -650,6 +651,31 @@ int buildGrid(ladds_gpu_ctx *c) {
   return LADDS_OK;
 }
 
+void freeGridBuffers(ladds_gpu_ctx *c) {
+  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->cellOff};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  c->rowStart = c->rowCounts = c->longRows = nullptr;
+  c->cellOff = nullptr;
+}
+
+// row tables of c->grid; the cell-offset table when it fits 1 GiB (250^3 cells: 31 MB)
+int allocGridBuffers(ladds_gpu_ctx *c) {
+  if (cudaMalloc(&c->rowStart, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->rowCounts, 2 * ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->longRows, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess) {
+    cudaGetLastError();
+    freeGridBuffers(c);
+    return fail(c, LADDS_ERR_ALLOC, "device allocation of the cell-row tables failed");
+  }
+  const size_t cellOffBytes = (size_t)c->nRows * cellOffPitch((uint32_t)c->grid.n[0]) * sizeof(uint16_t);
+  if (cellOffBytes <= ((size_t)1 << 30) && cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess) {
+    cudaGetLastError();
+    c->cellOff = nullptr;  // the scan then searches the sorted keys
+  }
+  return LADDS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -728,10 +754,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   c->cutF = (float)(f->cutoff * (1.0 + f->nearThresholdRel) * (1.0 + 1e-6));
   c->theta0 = gmstIAU1982(f->epochJD);
   if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&c->rowStart, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->rowCounts, 2 * ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->longRows, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
+      allocGridBuffers(c) != LADDS_OK || cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->dCount, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandCount, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
@@ -753,12 +776,6 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
   cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
-  // cell-offset table of the rows: used when it fits 1 GiB (250^3 cells: 31 MB)
-  const size_t cellOffBytes = (size_t)c->nRows * cellOffPitch((uint32_t)c->grid.n[0]) * sizeof(uint16_t);
-  if (cellOffBytes <= ((size_t)1 << 30) && cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess) {
-    cudaGetLastError();
-    c->cellOff = nullptr;  // the scan then searches the sorted keys
-  }
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);
   if (!rc) rc = ensureCandCapacity(c, (size_t)1 << 16);
@@ -965,7 +982,7 @@ int ladds_gpu_integrate(ladds_gpu_ctx *c, int steps) {
   CK(cudaSetDevice(c->dev));
   int left = steps;
   while (left > 0) {
-    const int chunk = std::min(left, kMaxEphSteps);
+    const int chunk = std::min(left, c->chunkSteps);
     CK(enqueueEphemeris(c, chunk));
     enqueuePropagate(c, chunk, false, 0);
     left -= chunk;
@@ -1101,7 +1118,7 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       const DevState cur0 = c->cur, alt0 = c->alt;
       uint32_t *const sk0 = c->sortedKeys, *const pm0 = c->perm;
       for (int done = 0; done < iterations;) {
-        const int len = std::min(iterations - done, kMaxEphSteps);
+        const int len = std::min(iterations - done, c->chunkSteps);
         const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
                                          c->pairCap);
         if (c->graphs.find(key) == c->graphs.end()) {
@@ -1126,7 +1143,7 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       // pass 2: replay
       CK(cudaEventRecord(c->callStart, c->st));
       for (int done = 0; done < iterations;) {
-        const int len = std::min(iterations - done, kMaxEphSteps);
+        const int len = std::min(iterations - done, c->chunkSteps);
         const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
                                          c->pairCap);
         auto git = c->graphs.find(key);
@@ -1138,7 +1155,7 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
     } else {
       CK(cudaEventRecord(c->callStart, c->st));
       for (int done = 0; done < iterations;) {
-        const int len = std::min(iterations - done, kMaxEphSteps);
+        const int len = std::min(iterations - done, c->chunkSteps);
         enqueueChunk(c, it0 + done, len, k);
         done += len;
       }
@@ -1343,6 +1360,144 @@ int ladds_gpu_functor_pairs(ladds_gpu_ctx *c, const ladds_scan_params *p, size_t
   if (recs.size() > cap || (!out && !recs.empty()))
     return fail(c, LADDS_ERR_CAPACITY, "output buffer too small for the pair records");
   if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
+  return LADDS_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Autotuner: cell size, block shapes and the captured chunk length.
+namespace {
+
+// one timed trial of `cfg` (+ chunk length) on a copy of c's population
+int tuneTrial(ladds_gpu_ctx *c, const ladds_gpu_config &cfg, int chunk, int steps, ladds_tune_trial &t) {
+  ladds_gpu_ctx *tc = nullptr;
+  int rc = ladds_gpu_create(&cfg, &tc);
+  if (rc) return fail(c, rc, "autotune: a trial context could not be created");
+  tc->chunkSteps = chunk;
+  rc = ensureCapacity(tc, c->n);
+  if (!rc && c->n) {
+    const cudaError_t e = copyState(c->cur, tc->cur, c->n, c->st);
+    if (e != cudaSuccess) rc = fail(c, LADDS_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (!rc && cudaStreamSynchronize(c->st) != cudaSuccess) rc = fail(c, LADDS_ERR_CUDA, "autotune: state copy");
+  if (!rc) {
+    tc->n = c->n;
+    rc = ladds_gpu_set_iteration(tc, c->hostIter);
+  }
+  std::vector<ladds_pair> recs((size_t)1 << 16);
+  ladds_step_stats st{};
+  for (int pass = 0; pass < 2 && !rc; ++pass) {  // warm-up (captures the graphs), then the timed run
+    const int n = pass == 0 ? std::min(steps, 2 * chunk) : steps;
+    size_t got = 0;
+    rc = ladds_gpu_step(tc, n, recs.data(), recs.size(), &got, &st);
+    if (rc == LADDS_ERR_CAPACITY) {
+      recs.resize(got);
+      rc = ladds_gpu_step(tc, n, recs.data(), recs.size(), &got, &st);
+    }
+    if (rc) rc = fail(c, rc, std::string("autotune trial: ") + ladds_gpu_last_error(tc));
+  }
+  if (!rc) {
+    t.cellSize = tc->grid.cellSize;
+    t.reach = tc->grid.reach;
+    t.propagateBlock = cfg.propagateBlock;
+    t.scanBlock = cfg.scanBlock;
+    t.chunkSteps = chunk;
+    t.msPerStep = st.deviceMs / std::max(steps, 1);
+  }
+  ladds_gpu_destroy(tc);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *trials, size_t cap, size_t *nTrials,
+                       ladds_tune_trial *best) {
+  if (!c || stepsPerTrial < 1 || !best || (cap && !trials)) return fail(c, LADDS_ERR_INVALID_ARG, "autotune: bad argument");
+  std::vector<ladds_tune_trial> all;
+  ladds_gpu_config cfg = c->cfg;
+  cfg.pairCapacity = c->pairCap;
+  cfg.useGraphs = 1;
+  ladds_tune_trial bestT{};
+  bestT.msPerStep = INFINITY;
+  int bestChunk = c->chunkSteps;
+  auto run = [&](const ladds_gpu_config &k, int chunk) -> int {
+    ladds_tune_trial t{};
+    const int rc = tuneTrial(c, k, chunk, stepsPerTrial, t);
+    if (rc) return rc;
+    all.push_back(t);
+    if (t.msPerStep < bestT.msPerStep) {
+      bestT = t;
+      cfg = k;
+      bestChunk = chunk;
+    }
+    return LADDS_OK;
+  };
+  // 1. cell edge in [20, 160] km: cutoff / R (neighbour reach R = 1..4) and
+  //    coarser cells 1.5 and 2 cutoffs wide (reach 1); the current edge as well
+  {
+    const ladds_gpu_config base = cfg;
+    std::vector<double> cells = {base.cellSize};
+    for (int R = 1; R <= 4; ++R) cells.push_back(base.cutoff * (1.0 + 1e-6) / R);
+    cells.push_back(1.5 * base.cutoff);
+    cells.push_back(2.0 * base.cutoff);
+    for (size_t i = 0; i < cells.size(); ++i) {
+      const double cs = cells[i];
+      if (i > 0 && (cs < 20.0 || cs > 160.0)) continue;
+      if (i == 1 && base.cellSize <= 0) continue;  // the default edge: measured as the current one
+      if (i > 1 && cs == base.cellSize) continue;
+      ladds_gpu_config k = base;
+      k.cellSize = cs;
+      const int rc = run(k, bestChunk);
+      if (rc) return rc;
+    }
+  }
+  // 2. block shapes of the propagation and of the pair evaluation
+  {
+    const ladds_gpu_config base = cfg;
+    for (int pb : {128, 256})
+      for (int sb : {128, 256}) {
+        ladds_gpu_config k = base;
+        k.propagateBlock = pb;
+        k.scanBlock = sb;
+        if ((pb == base.propagateBlock || (pb == 256 && base.propagateBlock == 0)) &&
+            (sb == base.scanBlock || (sb == 256 && base.scanBlock == 0)))
+          continue;  // measured already
+        const int rc = run(k, bestChunk);
+        if (rc) return rc;
+      }
+  }
+  // 3. iterations per captured chunk
+  {
+    const ladds_gpu_config base = cfg;
+    for (int chunk : {32, 64, 128}) {
+      if (chunk == bestChunk) continue;
+      const int rc = run(base, chunk);
+      if (rc) return rc;
+    }
+  }
+  // apply the best configuration to the context (its state is untouched)
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  CK(cudaSetDevice(c->dev));
+  CK(cudaStreamSynchronize(c->st));
+  const bool regrid = cfg.cellSize != c->cfg.cellSize;
+  c->cfg.cellSize = cfg.cellSize;
+  c->cfg.propagateBlock = cfg.propagateBlock;
+  c->cfg.scanBlock = cfg.scanBlock;
+  c->chunkSteps = bestChunk;
+  dropGraphs(c);
+  if (regrid) {
+    freeGridBuffers(c);
+    int rc = buildGrid(c);
+    if (!rc) rc = allocGridBuffers(c);
+    if (rc) return rc;
+    c->orderValid = false;
+  }
+  *best = bestT;
+  if (nTrials) *nTrials = all.size();
+  for (size_t i = 0; i < all.size() && i < cap; ++i) trials[i] = all[i];
   return LADDS_OK;
 }
 
