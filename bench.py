@@ -278,6 +278,29 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------ other workloads
+def workload_leg(capi, device, which, n, steps, tune):
+    """Throughput of population `which` (2: four constellation shells + debris,
+    4: small-debris mixture) with the full force set in split precision, scan
+    every step; optionally autotuned first (cell edge, block shapes, chunk)."""
+    pop = capi.generate_population(which, SEED + which, n)
+    out = {"population": which, "n_objects": n, "steps": steps}
+    with capi.Context(capi.default_config(componentMask=capi.PROP_ALL, precision=capi.PRECISION_SPLIT,
+                                          device=device, pairCapacity=1 << 18)) as ctx:
+        ctx.upload(pop)
+        ctx.step(4)
+        if tune:
+            best, trials = ctx.autotune(16)
+            out["autotuned"] = best
+            out["trials"] = len(trials)
+        ctx.step(8)
+        res = ctx.step(steps)
+        ms = res.stats.deviceMs
+        out.update({"value": n * steps / (ms * 1e-3), "unit": "object-steps/s", "ms_per_step": ms / steps,
+                    "records": int(res.stats.records), "collisions": int(res.stats.collisions)})
+    return out
+
+
 # ---------------------------------------------------------- adjoint leg
 def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
     """Differentiation workload: 4096 pairs, 1080 FP64 steps of the full force
@@ -340,6 +363,7 @@ def main():
     ap.add_argument("--no-drift", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--reference-budget", type=float, default=150.0)
     args = ap.parse_args()
@@ -384,6 +408,15 @@ def main():
         results[name]["phases"]["launches"] = {p: getattr(pt, p + "Launches") for p in capi.PhaseTimes.PHASES}
         ctx.set_profiling(False)
         ctx.close()
+
+    workloads = {}
+    if not args.no_workloads and rank == 0:
+        for name, which, n_obj, steps, tune in (("constellation_shells", 2, 2_004_224, 128, True),
+                                                 ("scale_8M", 4, 8_000_000, 32, False)):
+            try:
+                workloads[name] = workload_leg(capi, local, which, n_obj, steps, tune)
+            except Exception as ex:  # noqa: BLE001
+                workloads[name] = {"error": str(ex)[:200]}
 
     # one-day drift of split vs FP64 (both from the same start state)
     adjoint = None
@@ -520,6 +553,7 @@ def main():
         "drift": drift,
         "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
         "adjoint": adjoint,
+        "workloads": workloads,
         "records": {"split": split["records"], "fp64": fp64["records"]},
         "e2e": e2e,
         "roofline": roofline,

@@ -31,6 +31,22 @@ namespace ladds {
 constexpr int kLargeRow = 4096;  // objects sorted in shared memory by one CTA (48 KB)
 constexpr int kBucketThreads = 256;
 
+// Occupancy bin of the pair scan: cells holding at least minCount objects are
+// listed (key r * nx + ix) by the row sorts; their objects are scanned by cell
+// tiles (k_pair_tiles) instead of the per-object walk.  cells == nullptr: off.
+struct DenseBin {
+  uint32_t *cells;
+  uint32_t *count;
+  uint32_t cap;
+  uint32_t minCount;
+};
+constexpr uint32_t kDenseCell = 12;  // objects per cell from which the cell is scanned by tiles
+
+__device__ __forceinline__ void denseAppend(const DenseBin &d, uint32_t key) {
+  const uint32_t q = atomicAdd(d.count, 1u);
+  if (q < d.cap) d.cells[q] = key;
+}
+
 __device__ __forceinline__ uint32_t laneMaskLt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -267,7 +283,8 @@ __host__ __device__ __forceinline__ size_t rowSortSmem(uint32_t nx) {
 __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
     const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
     const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
-    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff) {
+    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff,
+    DenseBin dense) {
   extern __shared__ uint32_t smemRows[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t H = rowCountWords(nx), per = H / 32u;
@@ -309,10 +326,12 @@ __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
       if (lane >= o) incl += t;
     }
     uint32_t run = incl - sum;
+    const bool listDense = cellOff && dense.cells && L >= dense.minCount;
     for (uint32_t i = 0; i < per; ++i) {
-      const uint32_t c = hist[lane * per + i];
-      hist[lane * per + i] = run;
+      const uint32_t cc = lane * per + i, c = hist[cc];
+      hist[cc] = run;
       run += c;
+      if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + cc);  // cc < nx: counts past nx are 0
     }
     __syncwarp();
     if (cellOff) {
@@ -346,7 +365,7 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
     const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,
     uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
     const uint32_t *__restrict__ longRows, const uint32_t *__restrict__ longCount,
-    uint16_t *__restrict__ cellOff) {
+    uint16_t *__restrict__ cellOff, DenseBin dense) {
   extern __shared__ unsigned long long smem[];
   unsigned long long *sv = smem;
   uint32_t *sp = reinterpret_cast<uint32_t *>(smem + kLargeRow);
@@ -389,9 +408,14 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
       sortedKeys[s + i] = r * nx + (uint32_t)(V[i] >> 32);
       perm[s + i] = I[i];
     }
-    if (cellOff && L <= 65535u)  // offsets are 16-bit; longer rows are searched by the scan
-      fillCellOffsets(cellOff + (size_t)r * cellOffPitch(nx), nx, L,
-                      [&](uint32_t i) { return (uint32_t)(V[i] >> 32); }, threadIdx.x, blockDim.x);
+    if (cellOff && L <= 65535u) {  // offsets are 16-bit; longer rows are searched by the scan
+      uint16_t *t = cellOff + (size_t)r * cellOffPitch(nx);
+      fillCellOffsets(t, nx, L, [&](uint32_t i) { return (uint32_t)(V[i] >> 32); }, threadIdx.x, blockDim.x);
+      __syncthreads();
+      if (dense.cells)
+        for (uint32_t c = threadIdx.x; c < nx; c += blockDim.x)
+          if ((uint32_t)(t[c + 1] - t[c]) >= dense.minCount) denseAppend(dense, r * nx + c);
+    }
     __syncthreads();
   }
 }

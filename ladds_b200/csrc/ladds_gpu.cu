@@ -113,6 +113,8 @@ struct ladds_gpu_ctx {
   int evalBlocks = 592;     // grid of the candidate-evaluation kernel (4 per SM)
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
   int chunkSteps = kMaxEphSteps;  // iterations per ephemeris chunk / captured graph (autotuned)
+  uint32_t *denseCells = nullptr, *denseCount = nullptr;  // dense bin of the pair scan (cells >= kDenseCell)
+  uint32_t denseCap = 0;
   struct Adjoint {          // buffers of the adjoint pair batch (ladds_gpu_adjoint_*)
     size_t nPairs = 0;
     int steps = 0, ck = 0;
@@ -248,6 +250,14 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
       cudaMalloc(&c->blockSums, (scanBlocks + 1) * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
     return fail(c, LADDS_ERR_ALLOC, "device allocation failed (cell-order buffers)");
+  }
+  if (c->denseCells) cudaFree(c->denseCells);
+  c->denseCap = (uint32_t)(newCap / kDenseCell + 1);
+  if (cudaMalloc(&c->denseCells, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
+    cudaGetLastError();
+    c->denseCells = nullptr;
+    c->denseCap = 0;
+    return fail(c, LADDS_ERR_ALLOC, "device allocation failed (dense-cell list)");
   }
   c->cap = newCap;
   c->orderValid = false;
@@ -445,6 +455,13 @@ void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, ui
   k_scan_add<<<nb1, kScanBlock, 0, c->st>>>(out, (int)count, s1x);
 }
 
+// the dense bin of the pair scan: on with the counting row sort and the cell tables
+DenseBin denseBin(const ladds_gpu_ctx *c) {
+  const bool on = c->cellOff && c->denseCells && (uint32_t)c->grid.n[0] <= (uint32_t)kRowCountMaxNx &&
+                  c->grid.reach <= 3;  // k_pair_tiles: one lane per half-shell row (<= 25 rows)
+  return DenseBin{on ? c->denseCells : nullptr, c->denseCount, c->denseCap, kDenseCell};
+}
+
 // keys0 holds the keys of c->cur in current order, rowCounts their row counts
 // and scratchC their arrival indices (k_propagate<*, true> or k_cell_keys) ->
 // sortedKeys (keys1), perm (vals1) and the row-start table; order = sort by
@@ -455,22 +472,25 @@ void enqueueSort(ladds_gpu_ctx *c) {
   {
     PhaseScope ps(c, kPhBucket, c->st, 1 + exclusiveScanKernels((size_t)nRows + 1));
     cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
+    cudaMemsetAsync(c->denseCount, 0, sizeof(uint32_t), c->st);
     enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
     k_bucket_place<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
         c->keys0, c->scratchC, c->cur.tag, n, nx, c->rowStart, c->sortRec, c->vals0, c->dStatus);
   }
   PhaseScope ps(c, kPhRowsort, c->st, 2);
+  const DenseBin dense = denseBin(c);
   if (nx <= (uint32_t)kRowCountMaxNx) {  // counting sort inside the rows
     const int rowBlocks = std::min(blocksFor((size_t)nRows * 32, kRowSortThreads), 32 * c->evalBlocks);
     k_bucket_sort_rows<<<rowBlocks, kRowSortThreads, rowSortSmem(nx), c->st>>>(
-        c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
+        c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff,
+        dense);
   } else {
     const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 16 * c->evalBlocks);
     k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
         c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   }
   k_bucket_sort_large<<<c->evalBlocks / 2, kBucketThreads, kLargeRow * 12, c->st>>>(
-      c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
+      c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff, dense);
   c->sortedKeys = c->keys1;
   c->perm = c->vals1;
 }
@@ -495,12 +515,19 @@ inline float prefilterRadius(double cutoff, double nearRel) {
 // candidates + evaluation on stream s; records carry *iterPtr + iterOffset
 void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, float cutF, const int64_t *iterPtr,
                      int64_t iterOffset) {
+  const DenseBin dense = denseBin(c);
   {
-    PhaseScope ps(c, kPhCandidates, s);
+    PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
     cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), s);
     k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
         c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
-        sc.nearRel, cutF, c->dCand, c->dCandCount, (unsigned long long)c->candCap);
+        sc.nearRel, cutF, dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, c->dCand, c->dCandCount,
+        (unsigned long long)c->candCap);
+    if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
+      k_pair_tiles<<<4 * c->evalBlocks, kScanCta, 0, s>>>(dense.cells, dense.count, dense.cap, c->cur.tag, c->pos4,
+                                                      c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
+                                                      sc.cutoffSq, sc.nearRel, cutF, c->dCand, c->dCandCount,
+                                                      (unsigned long long)c->candCap);
   }
   PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
@@ -755,6 +782,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   c->theta0 = gmstIAU1982(f->epochJD);
   if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       allocGridBuffers(c) != LADDS_OK || cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->denseCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->dCount, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandCount, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
@@ -798,7 +826,8 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   dropGraphs(c);
   freeBuffers(c);
-  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->dCount, c->dStatus, c->dEph,
+  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->denseCount, c->denseCells, c->dCount,
+                  c->dStatus, c->dEph,
                   c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff, c->dObj,
                   c->adj.st, c->adj.bc, c->adj.aom, c->adj.miss, c->adj.grad, c->adj.ckpt, c->adj.rec,
                   c->adj.off, c->adj.arg, c->adj.eph};
@@ -1493,6 +1522,16 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
     int rc = buildGrid(c);
     if (!rc) rc = allocGridBuffers(c);
     if (rc) return rc;
+    if (c->cap) {  // the row-start scan's partial sums are sized by max(objects, rows)
+      const size_t scanLen = std::max(c->cap + 1, (size_t)c->nRows + 1);
+      const size_t wsWords = 4 * (scanLen / kScanBlock + 2) + 4 * kScanBlock;
+      if (c->scanWs) cudaFree(c->scanWs);
+      c->scanWs = nullptr;
+      if (cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, LADDS_ERR_ALLOC, "autotune: scan workspace");
+      }
+    }
     c->orderValid = false;
   }
   *best = bestT;
@@ -1903,8 +1942,8 @@ int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, 
     const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 64 * d.sms);
     k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, s>>>(rowStartS, nRows, nx, rec, src, sortedKeys, order,
                                                                longRows, longCount, nullptr);
-    k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(rowStartS, nx, rec, src, sortedKeys,
-                                                                          order, longRows, longCount, nullptr);
+    k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(
+        rowStartS, nx, rec, src, sortedKeys, order, longRows, longCount, nullptr, DenseBin{nullptr, nullptr, 0, 0});
   }
   if (rowStart) cudaMemcpyAsync(rowStart, rowStartS, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
   unsigned hostStatus = 0;

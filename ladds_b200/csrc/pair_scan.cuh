@@ -7,36 +7,23 @@
 // cell-offset table (written by the cell sort) instead of a search; rows whose
 // offsets do not fit 16 bits, or grids too large for the table, fall back to a
 // binary search on the sorted keys.  A binary32 distance test with a margin
-// larger than its rounding error rejects most candidates; the survivors get
-// the exact binary64 cutoff gate d^2 <= cutoff^2 (CollisionFunctor.cpp:71-77,
-// same rounding) or its near band.  Candidates are buffered per warp in shared
-// memory and appended with one global atomic per warp (no block barriers).
+// larger than its rounding error (and than the near band of the gate) keeps a
+// superset of the pairs within the cutoff.  Candidates are buffered per warp in
+// shared memory and appended with one global atomic per warp (no block
+// barriers).  Objects of cells with >= kDenseCell objects are sources of
+// k_pair_tiles instead (the occupancy bin of crowded cells).
 //
-// Phase 2, k_pair_eval: one thread per candidate evaluates the functor
-// (CollisionFunctor.cpp:40-131) and appends the records.
+// Phase 2, k_pair_eval: one thread per candidate applies the exact binary64
+// cutoff gate d^2 <= cutoff^2 (CollisionFunctor.cpp:71-77, same rounding) and
+// the functor (CollisionFunctor.cpp:40-131), and appends the records.
 #pragma once
-#include <cooperative_groups.h>
-
+#include "cell_sort.cuh"
 #include "conjunction.cuh"
 
 namespace ladds {
 
-namespace cg = cooperative_groups;
-
 constexpr int kScanCta = 128;
 constexpr int kWarpCand = 128;  // candidates buffered per warp before a global append
-
-// Direct global append (only for candidates beyond a warp's shared buffer).
-__device__ __forceinline__ void appendCandidateGlobal(uint32_t a, uint32_t b, uint2 *__restrict__ cand,
-                                                      unsigned long long *__restrict__ count,
-                                                      unsigned long long cap) {
-  cg::coalesced_group grp = cg::coalesced_threads();
-  unsigned long long base = 0;
-  if (grp.thread_rank() == 0) base = atomicAdd(count, (unsigned long long)grp.size());
-  base = grp.shfl(base, 0);
-  const unsigned long long pos = base + grp.thread_rank();
-  if (pos < cap) cand[pos] = make_uint2(a, b);
-}
 
 // [lo, hi) of the cells xlo..xhi of row r2 in the sorted arrays
 __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xhi, uint32_t nx,
@@ -59,28 +46,43 @@ __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xh
   }
 }
 
-// Binary32 pre-filter and exact binary64 gate of one candidate pair (j, k)
-// with its positions already loaded; survivors go to the warp's buffer.
-__device__ __forceinline__ void testCandidate(uint32_t j, uint32_t k, float4 mf, float4 q,
-                                              const double4 *__restrict__ pos4, double cutoffSq, double nearRel,
-                                              float cutF, uint2 *sCandW, uint32_t *sNW, uint2 *__restrict__ cand,
-                                              unsigned long long *__restrict__ candCount,
-                                              unsigned long long candCap) {
+// Binary32 pre-filter of one candidate pair with its positions loaded.  The
+// exact binary64 gate is left to the evaluation (functorPair), which loads both
+// records anyway: a gate here would stall the whole warp on two dependent
+// global loads for every pass.
+__device__ __forceinline__ bool prefilterPass(float4 mf, float4 q, float cutF) {
   const float dx = mf.x - q.x, dy = mf.y - q.y, dz = mf.z - q.z;
   const float lim = cutF + 2.0f * (mf.w + q.w);
-  if (dx * dx + dy * dy + dz * dz > lim * lim * 1.000001f) return;
-  const double4 me = pos4[j], o = pos4[k];
-  double d[3];
-  d[0] = __dsub_rn(me.x, o.x);
-  d[1] = __dsub_rn(me.y, o.y);
-  d[2] = __dsub_rn(me.z, o.z);
-  const double d2 = dot3rn(d, d);
-  if (d2 > cutoffSq && !nearBand(d2, cutoffSq, nearRel)) return;
-  const uint32_t slot = atomicAdd(sNW, 1u);  // shared counter: no global contention
-  if (slot < (uint32_t)kWarpCand)
-    sCandW[slot] = make_uint2(j, k);
-  else
-    appendCandidateGlobal(j, k, cand, candCount, candCap);
+  return !(dx * dx + dy * dy + dz * dz > lim * lim * 1.000001f);
+}
+
+// Per-warp candidate buffer in shared memory with its fill count n held in a
+// register (warp-uniform): appends are ballots, no atomics; a full buffer is
+// written out with one global atomic.  Every lane of the warp calls these.
+__device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, uint2 *__restrict__ cand,
+                                          unsigned long long *__restrict__ candCount, unsigned long long candCap) {
+  __syncwarp();
+  if (n) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(candCount, (unsigned long long)n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = (uint32_t)lane; i < n; i += 32u) {
+      const unsigned long long pos = base + i;
+      if (pos < candCap) cand[pos] = buf[i];
+    }
+    __syncwarp();
+  }
+  n = 0;
+}
+
+__device__ __forceinline__ void warpAppend(bool pass, uint32_t j, uint32_t k, int lane, uint2 *buf, uint32_t &n,
+                                           uint2 *__restrict__ cand, unsigned long long *__restrict__ candCount,
+                                           unsigned long long candCap) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, pass);
+  if (!mask) return;
+  if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) warpFlush(lane, buf, n, cand, candCount, candCap);
+  if (pass) buf[n + (uint32_t)__popc(mask & laneMaskLt())] = make_uint2(j, k);
+  n += (uint32_t)__popc(mask);
 }
 
 // owner lane of item t: the largest lane whose excl <= t (lanes with empty
@@ -100,9 +102,8 @@ __device__ __forceinline__ int windowOwner(uint32_t excl, uint32_t item) {
 // `excl`) and dealt out 32 items per round, so every lane tests one pair per
 // round however uneven the windows are.
 __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int lane, int warpBase,
-                                                const double4 *__restrict__ pos4, const float4 *__restrict__ posf,
-                                                double cutoffSq, double nearRel, float cutF, uint2 *sCandW,
-                                                uint32_t *sNW, uint2 *__restrict__ cand,
+                                                const float4 *__restrict__ posf, float cutF, uint2 *sCandW,
+                                                uint32_t &nBuf, uint2 *__restrict__ cand,
                                                 unsigned long long *__restrict__ candCount,
                                                 unsigned long long candCap) {
   const uint32_t cnt = hi - lo;
@@ -118,10 +119,9 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
     const uint32_t item = base + (uint32_t)lane;
     const int owner = windowOwner(excl, item);
     const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
-    if (item >= total) continue;
     const uint32_t jj = (uint32_t)(warpBase + owner), k = oLo + (item - oEx);
-    testCandidate(jj, k, __ldg(&posf[jj]), __ldg(&posf[k]), pos4, cutoffSq, nearRel, cutF, sCandW, sNW, cand,
-                  candCount, candCap);
+    const bool pass = item < total && prefilterPass(__ldg(&posf[jj]), __ldg(&posf[k]), cutF);
+    warpAppend(pass, jj, k, lane, sCandW, nBuf, cand, candCount, candCap);
   }
 }
 
@@ -135,19 +135,19 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
                                                               const uint32_t *__restrict__ rowStart,
                                                               const uint16_t *__restrict__ cellOff, GridDesc g,
                                                               double cutoffSq, double nearRel, float cutF,
+                                                              uint32_t denseMin,
+                                                              const uint32_t *__restrict__ denseCount,
                                                               uint2 *__restrict__ cand,
                                                               unsigned long long *__restrict__ candCount,
                                                               unsigned long long candCap) {
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
-  __shared__ uint32_t sN[kScanCta / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) sN[warp] = 0;
-  __syncwarp();
+  uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
   const int warpBase = blockIdx.x * kScanCta + warp * 32;
   const int j = warpBase + lane;
   const bool inRange = j < n;
   const uint32_t myTag = inRange ? tags[j] : kTagDummy;
-  const bool active = inRange && !tagDummy(myTag);
+  bool active = inRange && !tagDummy(myTag);
   const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
   int32_t ix = 0, iy = 0, iz = 0;
   if (active) {
@@ -156,6 +156,14 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
     const uint32_t row = key / (uint32_t)nx;
     iy = (int32_t)(row % (uint32_t)ny);
     iz = (int32_t)(row / (uint32_t)ny);
+    // objects of the dense bin (own cell >= denseMin objects) are scanned by k_pair_tiles
+    if (cellOff && denseMin != 0xffffffffu && __ldg(denseCount) != 0u) {
+      const uint32_t rs0 = __ldg(&rowStart[row]), rs1 = __ldg(&rowStart[row + 1]);
+      if (rs1 - rs0 <= 65535u) {
+        const uint16_t *t = cellOff + (size_t)row * cellOffPitch((uint32_t)nx);
+        if ((uint32_t)(__ldg(&t[ix + 1]) - __ldg(&t[ix])) >= denseMin) active = false;
+      }
+    }
   }
   const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
   for (int dz = 0; dz <= R; ++dz) {
@@ -173,21 +181,125 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
           rowWindow(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo, hi);
         }
       }
-      warpWindowPairs(lo, hi, lane, warpBase, pos4, posf, cutoffSq, nearRel, cutF, sCand[warp], &sN[warp], cand,
-                      candCount, candCap);
+      warpWindowPairs(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, cand, candCount, candCap);
     }
   }
-  // one global append per warp for its buffered candidates
-  __syncwarp();
-  const uint32_t m = min(sN[warp], (uint32_t)kWarpCand);
-  unsigned long long base = 0;
-  if (lane == 0 && m) base = atomicAdd(candCount, (unsigned long long)m);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  for (uint32_t i = lane; i < m; i += 32) {
-    const unsigned long long pos = base + i;
-    if (pos < candCap) cand[pos] = sCand[warp][i];
-  }
+  warpFlush(lane, sCand[warp], nBuf, cand, candCount, candCap);
 }
+
+// Dense bin of the pair scan (cells with >= kDenseCell objects, listed by the
+// row sorts): one warp per listed cell.  Lane q locates the window of
+// half-shell row q (the own row from the cell on; rows (dz, dy) > (0, 0) over
+// ix - R .. ix + R) -- all rows' lookups in flight together -- and the warp
+// stages up to kTileStage neighbour objects of the concatenated windows in
+// shared memory with independent loads.  Then every source lane (the cell's
+// objects, 32 at a time) tests every staged object: no per-pair address work,
+// no divergence but the survivors', no dependent global load inside the loop.
+// Own-row objects are paired with later objects only.  Same pre-filter and
+// candidate output as k_pair_candidates, which skips these objects as sources.
+constexpr uint32_t kTileStage = 256;  // staged neighbour objects per warp and pass
+
+__device__ __forceinline__ int halfShellRowOf(int q, int R, int &dz, int &dy) {
+  if (q <= R) {
+    dz = 0;
+    dy = q;
+  } else {
+    const int t = q - (R + 1);
+    dz = 1 + t / (2 * R + 1);
+    dy = t % (2 * R + 1) - R;
+  }
+  return q;
+}
+
+__global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restrict__ denseCells,
+                                                         const uint32_t *__restrict__ denseCount, uint32_t denseCap,
+                                                         const uint32_t *__restrict__ tags,
+                                                         const double4 *__restrict__ pos4,
+                                                         const float4 *__restrict__ posf,
+                                                         const uint32_t *__restrict__ skeys,
+                                                         const uint32_t *__restrict__ rowStart,
+                                                         const uint16_t *__restrict__ cellOff, GridDesc g,
+                                                         double cutoffSq, double nearRel, float cutF,
+                                                         uint2 *__restrict__ cand,
+                                                         unsigned long long *__restrict__ candCount,
+                                                         unsigned long long candCap) {
+  __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
+  __shared__ float4 sNb[kScanCta / 32][kTileStage];
+  __shared__ uint32_t sK[kScanCta / 32][kTileStage];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
+  const uint32_t nDense = min(*denseCount, denseCap);
+  const uint32_t gw = (blockIdx.x * kScanCta + threadIdx.x) >> 5, nW = (gridDim.x * kScanCta) >> 5;
+  const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
+  const int nq = (R + 1) + R * (2 * R + 1);  // half-shell rows (<= 32 for R <= 3)
+  const uint32_t pitch = cellOffPitch((uint32_t)nx);
+  for (uint32_t q = gw; q < nDense; q += nW) {
+    const uint32_t key = denseCells[q];
+    const uint32_t r = key / (uint32_t)nx;
+    const int32_t ix = (int32_t)(key - r * (uint32_t)nx), iy = (int32_t)(r % (uint32_t)ny),
+                  iz = (int32_t)(r / (uint32_t)ny);
+    const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
+    const uint32_t rs = __ldg(&rowStart[r]);
+    const uint16_t *t = cellOff + (size_t)r * pitch;
+    const uint32_t c0 = rs + __ldg(&t[ix]), c1 = rs + __ldg(&t[ix + 1]);
+    // lane q: window of half-shell row q
+    uint32_t lo = 0, hi = 0;
+    if (lane < nq) {
+      int dz, dy;
+      halfShellRowOf(lane, R, dz, dy);
+      const int32_t jz = iz + dz, jy = iy + dy;
+      if (jz < nz && jy >= 0 && jy < ny) {
+        if (lane == 0) {
+          lo = c0;
+          hi = rs + __ldg(&t[xhi + 1]);
+        } else {
+          rowWindow((uint32_t)jz * (uint32_t)ny + (uint32_t)jy, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys,
+                    lo, hi);
+        }
+      }
+    }
+    const uint32_t cnt = hi - lo;
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t excl = incl - cnt;
+    const uint32_t ownEnd = __shfl_sync(0xffffffffu, incl, 0);  // staged items [0, ownEnd) are own-row objects
+    for (uint32_t stBase = 0; stBase < total; stBase += kTileStage) {
+      const uint32_t m = min(kTileStage, total - stBase);
+      for (uint32_t ib = 0; ib < m; ib += 32u) {  // stage items stBase + i (warp-uniform loop)
+        const uint32_t i = ib + (uint32_t)lane, item = stBase + i;
+        // row of the item: the last lane whose excl <= item (empty rows share the next excl)
+        const int owner = windowOwner(excl, item);
+        const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
+        if (i < m) {
+          const uint32_t k = oLo + (item - oEx);
+          sNb[warp][i] = __ldg(&posf[k]);
+          sK[warp][i] = k;
+        }
+      }
+      __syncwarp();
+      for (uint32_t sBase = c0; sBase < c1; sBase += 32u) {
+        const uint32_t si = sBase + (uint32_t)lane;
+        const bool src = si < c1 && !tagDummy(tags[si]);
+        const float4 mf = src ? __ldg(&posf[si]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t u = 0; u < m; ++u) {  // warp-uniform
+          const float4 qq = sNb[warp][u];
+          const uint32_t k = sK[warp][u];
+          const bool pass = src && prefilterPass(mf, qq, cutF) &&
+                            !(stBase + u < ownEnd && k <= si);  // own row: later objects only
+          warpAppend(pass, si, k, lane, sCand[warp], nBuf, cand, candCount, candCap);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  warpFlush(lane, sCand[warp], nBuf, cand, candCount, candCap);
+}
+
 
 // grid-stride over the candidates (count read on the device)
 __global__ void __launch_bounds__(256) k_pair_eval(ScanPack pk, const uint2 *__restrict__ cand,

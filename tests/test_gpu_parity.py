@@ -144,6 +144,31 @@ def test_scan_bitexact_vs_oracle(capi, oracle, cell):
     assert np.array_equal(keys, okeys[operm])
 
 
+@pytest.mark.parametrize("cell", [0.0, 10.0])
+def test_scan_dense_cells_bitexact(capi, oracle, cell):
+    """Cells of hundreds of objects (the dense bin, scanned by cell tiles) next
+    to sparse cells (the per-object walk): records bit-exact vs the oracle."""
+    rng = np.random.default_rng(5)
+    parts = [dense_population(21, n=4000)]
+    for n_c, span, centre in ((3000, 30.0, (7010.0, 5.0, -3.0)), (600, 8.0, (6950.0, -40.0, 25.0)),
+                              (400, 2.0, (7100.0, 60.0, 60.0))):
+        c = dense_population(int(rng.integers(1 << 30)), n=n_c, span=span)
+        for k, off in zip("xyz", np.array(centre) - np.array([7000.0, 0.0, 0.0])):
+            c[k] = c[k] + off
+        parts.append(c)
+    pop = {k: np.concatenate([p_[k] for p_ in parts]) for k in parts[0]}
+    pop["id"] = np.arange(len(pop["x"]), dtype=np.uint64)
+    with ctx_for(capi, cellSize=cell, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(10.0)
+    p = oracle.scan_params(cutoff=20.0, dt=10.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    grid = oracle.make_grid(DENSE_BOX[0], DENSE_BOX[1], cell, 20.0)
+    ref = oracle.scan_cells(to_oracle(oracle, pop), p, grid)
+    assert len(ref) > 1000
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+
+
 @pytest.mark.parametrize("n,span", [(5000, 6.0), (3000, 40.0), (300, 60.0)])
 def test_cell_order_rows_of_every_length(capi, oracle, n, span):
     """Rows of > 4096, 33-256 and <= 32 objects take different sort paths
