@@ -35,6 +35,7 @@ struct ScanPack {
   double4 *vel4;      // vx, vy, vz, id (bit pattern)
   ulonglong2 *meta;   // parentId, tag
   float4 *posf;       // binary32 x, y, z + rounding bound
+  float4 *velf;       // binary32 vx, vy, vz + radius rounded up
 };
 
 __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n, ScanPack pk,
@@ -67,6 +68,7 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   pk.vel4[j] = make_double4(vx, vy, vz, __longlong_as_double((long long)id));
   pk.meta[j] = make_ulonglong2(parent, tag);
   pk.posf[j] = floatPosition(x, y, z);
+  pk.velf[j] = make_float4((float)vx, (float)vy, (float)vz, __double2float_ru(radius));
 }
 
 __device__ __forceinline__ double dot3rn(const double a[3], const double b[3]) {
@@ -166,6 +168,40 @@ __device__ __forceinline__ uint32_t functorPair(const ScanConsts &c, const Obj &
   if (!(dl2 > c.conjSq)) flags |= LADDS_PAIR_CONJUNCTION;
   if (nearBand(dl2, c.conjSq, c.nearRel)) flags |= LADDS_PAIR_NEAR_CONJUNCTION;
   return flags;
+}
+
+// Binary32 screen of a candidate pair: false only if the pair provably yields
+// no record, i.e. its closest approach over the step exceeds every threshold
+// (collision separation with the radii rounded up, evasion and conjunction
+// cutoffs, their near bands) and d^2 is outside the near band of the cutoff,
+// each by more than the error bound of this computation:
+//   positions: per-coordinate rounding <= posf.w (a 4x bound), velocities
+//   2^-24 |v| per coordinate, times dt; the closest approach over t is
+//   1-Lipschitz in the separation and dt-Lipschitz in the relative velocity;
+//   binary32 arithmetic on separations of size S: 2^-20 S.
+// NaN (identical velocities: the reference's 0/0 path) keeps the pair.
+__device__ __forceinline__ bool mayRecord(const ScanConsts &c, float4 pa, float4 va, float4 pb, float4 vb) {
+  const float dt = (float)c.dt;
+  const float drx = pa.x - pb.x, dry = pa.y - pb.y, drz = pa.z - pb.z;
+  const float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
+  const float ox = drx - dvx * dt, oy = dry - dvy * dt, oz = drz - dvz * dt;  // separation at the step start
+  const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+  float t = -(ox * dvx + oy * dvy + oz * dvz) / dv2;
+  t = (t < 0.0f) ? 0.0f : ((dt < t) ? dt : t);
+  const float mx = ox + dvx * t, my = oy + dvy * t, mz = oz + dvz * t;
+  const float dl = sqrtf(mx * mx + my * my + mz * mz);
+  const float d2 = drx * drx + dry * dry + drz * drz;
+  const float vmax = fmaxf(fmaxf(fabsf(va.x), fabsf(va.y)), fabsf(va.z)) +
+                     fmaxf(fmaxf(fabsf(vb.x), fabsf(vb.y)), fabsf(vb.z));
+  const float sepScale = sqrtf(d2) + sqrtf(dv2) * dt;
+  const float err = 3.5f * (pa.w + pb.w) + 3.5e-7f * vmax * dt + 1e-6f * sepScale + 1e-6f;
+  const float rel = 1.0f + 4.0f * (float)c.nearRel + 1e-6f;
+  const float sep = (va.w + vb.w) * (float)c.factor;
+  const float thr = fmaxf(fmaxf(sep, sqrtf((float)c.evasionSq)), sqrtf((float)c.conjSq)) * rel;
+  if (!(dl > thr + err)) return true;  // also NaN
+  // near band of the cutoff gate: |d^2 - cutoff^2| <= nearRel cutoff^2
+  const float cut2 = (float)c.cutoffSq, d2err = 2.0f * sqrtf(cut2) * err + 1e-5f * cut2;
+  return fabsf(d2 - cut2) <= cut2 * (float)c.nearRel * 1.01f + d2err;
 }
 
 __device__ __forceinline__ uint32_t lowerBound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi, uint32_t v) {

@@ -83,6 +83,7 @@ struct ladds_gpu_ctx {
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
   float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
   double4 *vel4 = nullptr;                // vx, vy, vz, id of the cell order
+  float4 *velf = nullptr;                 // binary32 velocities + radius of the cell order
   ulonglong2 *meta = nullptr;             // parentId, tag of the cell order
   uint32_t *rowStart = nullptr;
   uint32_t nRows = 0;
@@ -187,12 +188,13 @@ void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->alt);
   freeState(c->snap);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs, c->vel4, c->meta};
+                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs, c->vel4, c->meta, c->velf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c->pos4 = nullptr;
   c->posf = nullptr;
   c->vel4 = nullptr;
+  c->velf = nullptr;
   c->meta = nullptr;
   c->sortRec = nullptr;
   c->scanWs = nullptr;
@@ -244,6 +246,7 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   if (cudaMalloc(&c->pos4, newCap * sizeof(double4)) != cudaSuccess ||
       cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&c->vel4, newCap * sizeof(double4)) != cudaSuccess ||
+      cudaMalloc(&c->velf, newCap * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&c->meta, newCap * sizeof(ulonglong2)) != cudaSuccess ||
       cudaMalloc(&c->sortRec, newCap * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess ||
@@ -495,7 +498,7 @@ void enqueueSort(ladds_gpu_ctx *c) {
   c->perm = c->vals1;
 }
 
-inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf}; }
+inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf, c->velf}; }
 
 // gathers the state into cell order (so that the next propagation, key pass and
 // gather read nearly sequentially: objects move about one cell per step) and

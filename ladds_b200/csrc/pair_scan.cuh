@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(256) k_pair_eval(ScanPack pk, const uint2 *__r
   for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < m;
        q += (unsigned long long)gridDim.x * blockDim.x) {
     const uint2 p = cand[q];
+    if (!mayRecord(c, pk.posf[p.x], pk.velf[p.x], pk.posf[p.y], pk.velf[p.y])) continue;
     Obj a, b;
     loadObjPacked(pk, p.x, a);
     loadObjPacked(pk, p.y, b);
