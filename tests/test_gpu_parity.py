@@ -392,3 +392,53 @@ def test_clear_parents(capi):
         ctx.upload(pop)
         ctx.clear_parents()
         assert np.all(ctx.download()["parent"] == capi.SIZE_MAX)
+
+
+@pytest.mark.parametrize("near_rel", [1e-9, 1e-6])
+def test_threshold_neighbourhood_records_bitexact(capi, oracle, near_rel):
+    """Pairs whose closest approach sits within 1e-6 relative of the collision,
+    evasion or conjunction threshold, and pairs at the cutoff itself: the
+    evaluation's binary32 screen must keep every pair that yields a record
+    (near-band flags included); records bit-exact vs the oracle."""
+    rng = np.random.default_rng(17)
+    n_pairs = 900
+    dt = 10.0
+    radii = np.exp(rng.uniform(np.log(0.05), np.log(3.0), size=(n_pairs, 2)))
+    acts = rng.choice([0, 0, 1, 2], size=(n_pairs, 2)).astype(np.int8)
+    factor = 2000.0
+    sep = (radii[:, 0] + radii[:, 1]) * factor / 1000.0
+    kind = np.arange(n_pairs) % 4
+    thr = np.where(kind == 0, sep, np.where(kind == 1, 3.0, np.where(kind == 2, 2.0, 20.0)))
+    target = thr * (1.0 + rng.uniform(-2e-6, 2e-6, n_pairs))
+    rs, vs = [], []
+    for p in range(n_pairs):
+        ra = np.array([6600.0 + 45.0 * (p % 20), -450.0 + 45.0 * ((p // 20) % 20), -450.0 + 45.0 * (p // 400)])
+        va = rng.normal(size=3)
+        va *= 7.5 / np.linalg.norm(va)
+        dv = rng.normal(size=3)
+        dv *= rng.uniform(0.5, 12.0) / np.linalg.norm(dv)
+        if kind[p] == 3:  # at the cutoff: separation now, no relative motion along it
+            m = rng.normal(size=3)
+            m *= target[p] / np.linalg.norm(m)
+            rb = ra - m
+        else:  # closest approach inside the step, perpendicular to dv
+            m = np.cross(dv, rng.normal(size=3))
+            m *= target[p] / np.linalg.norm(m)
+            rb = ra - m - dv * (dt * rng.uniform(0.2, 0.8))
+        rs += [ra, rb]
+        vs += [va, va - dv]
+    ids = list(range(2 * n_pairs))
+    pop = from_lists(rs, vs, ids, acts.reshape(-1).tolist(), [1.0] * (2 * n_pairs), radii.reshape(-1).tolist())
+    kw = dict(DENSE_KW)
+    with ctx_for(capi, nearThresholdRel=near_rel, **kw) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(dt)
+    p = oracle.scan_params(cutoff=20.0, dt=dt, factor=factor, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0, near_rel=near_rel)
+    grid = oracle.make_grid(DENSE_BOX[0], DENSE_BOX[1], 0.0, 20.0)
+    ref = oracle.scan_cells(to_oracle(oracle, pop), p, grid)
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+    assert len(ref) > 150  # about half of the pairs sit just inside a threshold
+    if near_rel >= 1e-6:
+        near = capi.PAIR_NEAR_COLLISION | capi.PAIR_NEAR_EVASION | capi.PAIR_NEAR_CONJUNCTION | capi.PAIR_NEAR_GATE
+        assert np.sum((ref["flags"] & near) != 0) > 50
