@@ -283,6 +283,24 @@ typedef struct {
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
 
+/* ---- conjunction record output (host functions) ----
+ * The reference writes conjunctions as CSV (io/ConjuctionLogger.cpp:13-47:
+ * header "Iteration,P1,P2,SquaredDistance", one line per pair with the
+ * shortest round-trip decimal of dl2) or as HDF5 compound records
+ * {unsigned idA, unsigned idB, float distanceSquared} per iteration
+ * (io/hdf5/HDF5Definitions.h:42-68, HDF5Writer.cpp:151-188). */
+typedef struct {
+  uint32_t idA, idB;     /* Particle ids narrowed to unsigned int, as the reference does */
+  float distanceSquared; /* dl2 narrowed to float                                       */
+} ladds_collision_info;  /* 12 bytes: the HDF5 CollisionInfo / EvasionInfo layout      */
+/* Records with (flags & flagMask) != 0, in order, packed into the HDF5 layout.
+ * *nOut = their number; LADDS_ERR_CAPACITY if cap is smaller (out holds the first cap). */
+int ladds_records_pack(const ladds_pair *recs, size_t n, uint32_t flagMask, ladds_collision_info *out, size_t cap,
+                       size_t *nOut);
+/* Appends (append != 0) or writes the records with (flags & flagMask) != 0 as
+ * CSV lines "step,idA,idB,dl2"; the header is written when the file is empty. */
+int ladds_records_write_csv(const char *path, int append, const ladds_pair *recs, size_t n, uint32_t flagMask);
+
 /* ---- autotuner ----
  * No counterpart in the reference (its AutoPas container tunes its own
  * traversal).  Times trials of the context's step on a copy of its population

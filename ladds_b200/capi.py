@@ -83,8 +83,12 @@ EXPORTED = [
     "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
-    "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune",
+    "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
+    "ladds_records_write_csv",
 ]
+
+COLLISION_INFO_DTYPE = np.dtype([("idA", "<u4"), ("idB", "<u4"), ("distanceSquared", "<f4")])
+assert COLLISION_INFO_DTYPE.itemsize == 12
 
 ADJ_PAIR_DTYPE = np.dtype([("rA", "<f8", (3,)), ("vA", "<f8", (3,)), ("rB", "<f8", (3,)), ("vB", "<f8", (3,)),
                            ("bcInvA", "<f8"), ("bcInvB", "<f8"), ("aomA", "<f8"), ("aomB", "<f8")])
@@ -152,6 +156,8 @@ def lib():
     L.ladds_gpu_adjoint_forward.argtypes = [vp, vp, sz, i, i, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_backward.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_make_pairs.argtypes = [vp, C.c_uint64, sz, i, vp, vp]
+    L.ladds_records_pack.argtypes = [vp, sz, C.c_uint32, vp, sz, C.POINTER(sz)]
+    L.ladds_records_write_csv.argtypes = [C.c_char_p, i, vp, sz, C.c_uint32]
     L.ladds_gpu_autotune.argtypes = [vp, i, C.POINTER(TuneTrial), sz, C.POINTER(sz), C.POINTER(TuneTrial)]
     L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
@@ -440,3 +446,22 @@ class Context:
         t = PhaseTimes()
         self._check(self._L.ladds_gpu_phase_times(self._h, C.byref(t)))
         return t
+
+
+def pack_records(records: np.ndarray, flag_mask: int) -> np.ndarray:
+    """Records with (flags & flag_mask) in the HDF5 CollisionInfo layout (idA, idB as u32, dl2 as f32)."""
+    records = np.ascontiguousarray(records, dtype=PAIR_DTYPE)
+    out = np.zeros(max(len(records), 1), dtype=COLLISION_INFO_DTYPE)
+    n = C.c_size_t()
+    rc = lib().ladds_records_pack(_p(records), len(records), flag_mask, _p(out), len(out), C.byref(n))
+    if rc:
+        raise LaddsError(rc, "ladds_records_pack failed")
+    return out[: n.value].copy()
+
+
+def write_records_csv(path: str, records: np.ndarray, flag_mask: int, append: bool = False) -> None:
+    """CSV "Iteration,P1,P2,SquaredDistance" of the records with (flags & flag_mask)."""
+    records = np.ascontiguousarray(records, dtype=PAIR_DTYPE)
+    rc = lib().ladds_records_write_csv(path.encode(), 1 if append else 0, _p(records), len(records), flag_mask)
+    if rc:
+        raise LaddsError(rc, f"ladds_records_write_csv({path}) failed")
