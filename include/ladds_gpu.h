@@ -150,6 +150,18 @@ int ladds_gpu_upload(ladds_gpu_ctx *ctx, size_t n, const double *x, const double
 int ladds_gpu_append(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
                      const double *vx, const double *vy, const double *vz, const double *radius, const double *aom,
                      const double *bcInv, const uint64_t *id, const uint64_t *parentId, const int8_t *activity);
+/* Simulation::checkedInsert (Simulation.cpp:475-507): satellite i (arrays as
+ * for ladds_gpu_append) is appended only if no particle of the population --
+ * nor a satellite of this batch accepted before it -- lies in the half-open
+ * box [p - c, p + c) with dot(p - q, p - q) <= c^2, c = constellationCutoff
+ * (io/constellationCutoff).  delayed[i] = 1 for the satellites not inserted
+ * (the reference's delayedInsertion list); *nInserted (may be NULL) = the
+ * number appended.  Deleted objects do not block. */
+int ladds_gpu_checked_insert(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
+                             const double *vx, const double *vy, const double *vz, const double *radius,
+                             const double *aom, const double *bcInv, const uint64_t *id, const uint64_t *parentId,
+                             const int8_t *activity, double constellationCutoff, uint8_t *delayed,
+                             size_t *nInserted);
 /* Copies the population back in slot order.  Any array pointer may be NULL. */
 int ladds_gpu_download(ladds_gpu_ctx *ctx, size_t cap, size_t *n, double *x, double *y, double *z, double *vx,
                        double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,

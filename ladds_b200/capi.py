@@ -84,7 +84,7 @@ EXPORTED = [
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
-    "ladds_records_write_csv",
+    "ladds_records_write_csv", "ladds_gpu_checked_insert",
 ]
 
 COLLISION_INFO_DTYPE = np.dtype([("idA", "<u4"), ("idB", "<u4"), ("distanceSquared", "<f4")])
@@ -156,6 +156,7 @@ def lib():
     L.ladds_gpu_adjoint_forward.argtypes = [vp, vp, sz, i, i, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_backward.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_make_pairs.argtypes = [vp, C.c_uint64, sz, i, vp, vp]
+    L.ladds_gpu_checked_insert.argtypes = [vp, sz] + [vp] * 12 + [C.c_double, vp, C.POINTER(sz)]
     L.ladds_records_pack.argtypes = [vp, sz, C.c_uint32, vp, sz, C.POINTER(sz)]
     L.ladds_records_write_csv.argtypes = [C.c_char_p, i, vp, sz, C.c_uint32]
     L.ladds_gpu_autotune.argtypes = [vp, i, C.POINTER(TuneTrial), sz, C.POINTER(sz), C.POINTER(TuneTrial)]
@@ -400,6 +401,17 @@ class Context:
                 continue
             self._check(rc)
             return out[: n.value].copy()
+
+    def checked_insert(self, pop: dict, constellation_cutoff: float) -> np.ndarray:
+        """Simulation::checkedInsert: appends the satellites of `pop` that have no
+        particle within the cutoff; returns the delayed flags (1 = not inserted)."""
+        pop = as_population(pop)
+        n = len(pop["x"])
+        delayed = np.zeros(max(n, 1), dtype=np.uint8)
+        got = C.c_size_t()
+        self._check(self._L.ladds_gpu_checked_insert(self._h, n, *[_p(pop[k]) for k in POP_FIELDS],
+                                                     constellation_cutoff, _p(delayed), C.byref(got)))
+        return delayed[:n].copy()
 
     def autotune(self, steps_per_trial: int = 16):
         """Times cell edges, block shapes and chunk lengths; applies the fastest.

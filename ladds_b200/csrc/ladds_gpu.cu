@@ -28,6 +28,7 @@
 #include "pair_scan.cuh"
 #include "propagate.cuh"
 #include "adjoint.cuh"
+#include "insert.cuh"
 #include "population.h"
 
 using namespace ladds;
@@ -891,6 +892,77 @@ int ladds_gpu_append(ladds_gpu_ctx *c, size_t n, const double *x, const double *
   c->orderValid = false;
   dropGraphs(c);
   return LADDS_OK;
+}
+
+int ladds_gpu_checked_insert(ladds_gpu_ctx *c, size_t n, const double *x, const double *y, const double *z,
+                             const double *vx, const double *vy, const double *vz, const double *radius,
+                             const double *aom, const double *bcInv, const uint64_t *id, const uint64_t *parentId,
+                             const int8_t *activity, double constellationCutoff, uint8_t *delayed,
+                             size_t *nInserted) {
+  if (!c || (n && (!x || !y || !z || !id || !delayed)) || !(constellationCutoff >= 0.0))
+    return fail(c, LADDS_ERR_INVALID_ARG, "checked_insert: bad argument");
+  if (nInserted) *nInserted = 0;
+  if (!n) return LADDS_OK;
+  const double cc = constellationCutoff, c2 = cc * cc;
+  std::vector<uint8_t> blocked(n, 0);
+  {
+    std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+    CK(cudaSetDevice(c->dev));
+    if (c->n) {
+      double *dp = nullptr;
+      uint8_t *db = nullptr;
+      if (cudaMalloc(&dp, 3 * n * sizeof(double)) != cudaSuccess || cudaMalloc(&db, n) != cudaSuccess) {
+        cudaGetLastError();
+        if (dp) cudaFree(dp);
+        return fail(c, LADDS_ERR_ALLOC, "checked_insert: staging allocation failed");
+      }
+      cudaError_t e = cudaMemcpyAsync(dp, x, n * sizeof(double), cudaMemcpyHostToDevice, c->st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dp + n, y, n * sizeof(double), cudaMemcpyHostToDevice, c->st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dp + 2 * n, z, n * sizeof(double), cudaMemcpyHostToDevice, c->st);
+      if (e == cudaSuccess) {
+        k_insert_blocked<<<blocksFor(n * 32, 128), 128, 0, c->st>>>(c->cur, (int)c->n, dp, dp + n, dp + 2 * n,
+                                                                     (int)n, cc, c2, db);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaMemcpyAsync(blocked.data(), db, n, cudaMemcpyDeviceToHost, c->st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+      cudaFree(dp);
+      cudaFree(db);
+      if (e != cudaSuccess) return fail(c, LADDS_ERR_CUDA, std::string("checked_insert: ") + cudaGetErrorString(e));
+    }
+  }
+  // satellites of the batch, in order, against the ones accepted before them
+  std::vector<size_t> acc;
+  for (size_t i = 0; i < n; ++i) {
+    bool hit = blocked[i] != 0;
+    const double p[3] = {x[i], y[i], z[i]};
+    for (size_t q = 0; q < acc.size() && !hit; ++q) {
+      const double o[3] = {x[acc[q]], y[acc[q]], z[acc[q]]};
+      hit = insertBlocks(p, o, cc, c2);
+    }
+    delayed[i] = hit ? 1 : 0;
+    if (!hit) acc.push_back(i);
+  }
+  if (acc.empty()) return LADDS_OK;
+  const size_t m = acc.size();
+  std::vector<double> d[9];
+  const double *src[9] = {x, y, z, vx, vy, vz, radius, aom, bcInv};
+  for (int k = 0; k < 9; ++k) {
+    d[k].resize(m);
+    for (size_t q = 0; q < m; ++q) d[k][q] = src[k] ? src[k][acc[q]] : 0.0;
+  }
+  std::vector<uint64_t> ids(m), parents(m);
+  std::vector<int8_t> acts(m);
+  for (size_t q = 0; q < m; ++q) {
+    ids[q] = id[acc[q]];
+    parents[q] = parentId ? parentId[acc[q]] : UINT64_MAX;
+    acts[q] = activity ? activity[acc[q]] : (int8_t)LADDS_PASSIVE;
+  }
+  const int rc = ladds_gpu_append(c, m, d[0].data(), d[1].data(), d[2].data(), d[3].data(), d[4].data(),
+                                  d[5].data(), d[6].data(), d[7].data(), d[8].data(), ids.data(), parents.data(),
+                                  acts.data());
+  if (!rc && nInserted) *nInserted = m;
+  return rc;
 }
 
 int ladds_gpu_download(ladds_gpu_ctx *c, size_t cap, size_t *nOut, double *x, double *y, double *z, double *vx,

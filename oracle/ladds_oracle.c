@@ -822,3 +822,41 @@ void oracle_pair_losses(size_t nPairs, const double *pairs, const double *dirs, 
   }
   free(eph);
 }
+
+/* Simulation::checkedInsert, Simulation.cpp:475-507: satellite i is inserted
+ * if no particle in the region iterator's box [p - c, p + c) (AutoPas inBox:
+ * low <= q < high, corners from ArrayMath::sub / add) has
+ * dot(p - q, p - q) <= c^2 (collisionFree = dot > c^2); inserted satellites
+ * take part in the tests of the later ones (they are in the container). */
+static int insert_blocks(const double p[3], const double q[3], double c, double c2) {
+  for (int k = 0; k < 3; ++k) {
+    const double lo = p[k] - c, hi = p[k] + c;
+    if (!(q[k] >= lo && q[k] < hi)) return 0;
+  }
+  const double d[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+  return !(dot3(d, d) > c2);
+}
+
+size_t oracle_checked_insert(size_t nExisting, const double *ex, const double *ey, const double *ez,
+                             const uint8_t *dummy, size_t nNew, const double *nx, const double *ny,
+                             const double *nz, double cutoff, uint8_t *delayed) {
+  const double c2 = cutoff * cutoff;
+  size_t inserted = 0;
+  for (size_t i = 0; i < nNew; ++i) {
+    const double p[3] = {nx[i], ny[i], nz[i]};
+    int hit = 0;
+    for (size_t j = 0; j < nExisting && !hit; ++j) {
+      if (dummy && dummy[j]) continue;
+      const double q[3] = {ex[j], ey[j], ez[j]};
+      hit = insert_blocks(p, q, cutoff, c2);
+    }
+    for (size_t j = 0; j < i && !hit; ++j) {
+      if (delayed[j]) continue;
+      const double q[3] = {nx[j], ny[j], nz[j]};
+      hit = insert_blocks(p, q, cutoff, c2);
+    }
+    delayed[i] = (uint8_t)hit;
+    inserted += !hit;
+  }
+  return inserted;
+}

@@ -162,6 +162,12 @@ void oracle_propagate(size_t n, double *x, double *y, double *z, double *vx, dou
                       uint32_t mask, double jdEpoch, double t0, double dt, int steps, int nthreads);
 double oracle_density(double hKm);
 
+/* --- Simulation::checkedInsert (Simulation.cpp:475-507) --- delayed[i] = 1 for the
+ * new satellites not inserted; returns the number inserted. */
+size_t oracle_checked_insert(size_t nExisting, const double *ex, const double *ey, const double *ez,
+                             const uint8_t *dummy, size_t nNew, const double *nx, const double *ny,
+                             const double *nz, double cutoff, uint8_t *delayed);
+
 /* --- differentiation checks ---
  * Pair loss restated in tangent-linear (dual-number) arithmetic.  pairs: 16
  * doubles per pair (rA, vA, rB, vB, bcInvA, bcInvB, aomA, aomB); passive

@@ -104,6 +104,9 @@ def lib():
             C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
         L.oracle_pair_losses.argtypes = [C.c_size_t, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_double,
                                          C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.oracle_checked_insert.restype = C.c_size_t
+        L.oracle_checked_insert.argtypes = [C.c_size_t] + [C.c_void_p] * 4 + [C.c_size_t] + [C.c_void_p] * 3 + [
+            C.c_double, C.c_void_p]
         L.oracle_density.restype = C.c_double
         L.oracle_density.argtypes = [C.c_double]
         _lib = L
@@ -248,3 +251,14 @@ def pair_losses(pairs, steps, dt=10.0, mask=FULL, dirs=None, t0=0.0, jd_epoch=JD
     lib().oracle_pair_losses(n, _ptr(pairs), _ptr(d), mask, jd_epoch, t0, dt, steps, _ptr(miss), _ptr(tca),
                              _ptr(dmiss), nthreads)
     return miss, tca, dmiss
+
+
+def checked_insert(existing_xyz, new_xyz, cutoff, dummy=None):
+    """Simulation::checkedInsert restated: delayed flags of the new satellites."""
+    ex = [np.ascontiguousarray(a, dtype=np.float64) for a in existing_xyz]
+    nw = [np.ascontiguousarray(a, dtype=np.float64) for a in new_xyz]
+    delayed = np.zeros(len(nw[0]), dtype=np.uint8)
+    d = None if dummy is None else np.ascontiguousarray(dummy, dtype=np.uint8)
+    lib().oracle_checked_insert(len(ex[0]), _ptr(ex[0]), _ptr(ex[1]), _ptr(ex[2]), _ptr(d), len(nw[0]),
+                                _ptr(nw[0]), _ptr(nw[1]), _ptr(nw[2]), cutoff, _ptr(delayed))
+    return delayed
