@@ -279,7 +279,7 @@ def run_reference(args, world, rank):
 
 
 # ------------------------------------------------------ other workloads
-def workload_leg(capi, device, which, n, steps, tune):
+def workload_leg(capi, device, which, n, steps, tune, breakup_steps=0):
     """Throughput of population `which` (2: four constellation shells + debris,
     4: small-debris mixture) with the full force set in split precision, scan
     every step; optionally autotuned first (cell edge, block shapes, chunk)."""
@@ -298,6 +298,18 @@ def workload_leg(capi, device, which, n, steps, tune):
         ms = res.stats.deviceMs
         out.update({"value": n * steps / (ms * 1e-3), "unit": "object-steps/s", "ms_per_step": ms / steps,
                     "records": int(res.stats.records), "collisions": int(res.stats.collisions)})
+        if breakup_steps:
+            # breakups on the host after every iteration, fragments appended on the device
+            cfg = capi.BreakupConfig(0.05, 1, 2.2)
+            next_id = n
+            total_b = total_f = 0
+            for it in range(breakup_steps):
+                r = ctx.step(1)
+                nb, nf, next_id = ctx.breakup(r.records, cfg, 1000 + it, next_id)
+                total_b += nb
+                total_f += nf
+            out["breakup_run"] = {"iterations": breakup_steps, "breakups": total_b, "fragments": total_f,
+                                  "objects_after": ctx.size()}
     return out
 
 
@@ -411,10 +423,10 @@ def main():
 
     workloads = {}
     if not args.no_workloads and rank == 0:
-        for name, which, n_obj, steps, tune in (("constellation_shells", 2, 2_004_224, 128, True),
-                                                 ("scale_8M", 4, 8_000_000, 32, False)):
+        for name, which, n_obj, steps, tune, brk in (("constellation_shells", 2, 2_004_224, 128, True, 0),
+                                                      ("scale_8M", 4, 8_000_000, 32, True, 16)):
             try:
-                workloads[name] = workload_leg(capi, local, which, n_obj, steps, tune)
+                workloads[name] = workload_leg(capi, local, which, n_obj, steps, tune, brk)
             except Exception as ex:  # noqa: BLE001
                 workloads[name] = {"error": str(ex)[:200]}
 

@@ -295,6 +295,57 @@ typedef struct {
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
 
+/* ---- objects by slot ---- */
+typedef struct {
+  double r[3], v[3];  /* position [km], velocity [km/s] */
+  double radius;      /* [m] */
+  double aom;         /* [km^2/kg]; mass = pi radius^2 1e-6 / aom */
+  double bcInv;       /* [m^2/kg] */
+  uint64_t id, parentId;
+  int32_t activity;
+  uint32_t deleted;   /* 1: marked deleted (ladds_gpu_mark_deleted) */
+} ladds_state_record; /* 96 bytes */
+/* Current state of the objects with the given slots (upload / append index),
+ * in the order asked; LADDS_ERR_INVALID_ARG if a slot does not exist. */
+int ladds_gpu_get_objects(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t m, ladds_state_record *out);
+
+/* ---- breakups on the host (the NASA standard breakup model, collisions) ----
+ * The reference hands each collision to the external esa/NASA-breakup-model-cpp
+ * (BreakupWrapper.cpp:14-45), which is not in the tree.  This is a restatement
+ * of the published model (Johnson et al. 2001, NASA standard breakup model,
+ * collision case): catastrophic when the projectile's kinetic energy over the
+ * target mass reaches 40 J/g; N(>Lc) = 0.1 M^0.75 Lc^-1.71 fragments with
+ * M = mt + mp (catastrophic) or mp v^2 (v in km/s); Lc from that power law in
+ * [minLc, 2 max(radius)]; area-to-mass ratio from the spacecraft distributions
+ * (bi-normal above 11 cm, normal below 8 cm, either in between); area from
+ * Lc; delta-v log-normal with mean 0.9 log10(A/m) + 2.9 and sigma 0.4 [m/s] in
+ * a uniform random direction, added to the velocity of the parent the
+ * fragment is drawn from (by mass); every fragment at the collision point.
+ * With enforceMassConservation the fragments past the parents' total mass are
+ * dropped. */
+typedef struct {
+  double minLc;                    /* sim/breakup/minLc [m] (reference default 0.01) */
+  int32_t enforceMassConservation; /* sim/breakup/enforceMassConservation            */
+  double coefficientOfDrag;        /* sim/prop/coefficientOfDrag: bcInv = Cd A / m    */
+} ladds_breakup_config;
+/* Fragments of one collision of a and b at `point`: ids from *nextId (advanced),
+ * parentId for all fragments (spawn protection), passive.  Writes up to cap
+ * fragments to the SoA arrays; *nOut = the number of fragments (LADDS_ERR_CAPACITY
+ * if above cap).  Deterministic in seed. */
+int ladds_breakup_collision(const ladds_breakup_config *cfg, uint64_t seed, const ladds_state_record *a,
+                            const ladds_state_record *b, const double point[3], uint64_t parentId, uint64_t *nextId,
+                            size_t cap, size_t *nOut, double *x, double *y, double *z, double *vx, double *vy,
+                            double *vz, double *radius, double *aom, double *bcInv, uint64_t *id, uint64_t *parent,
+                            int8_t *activity);
+/* BreakupWrapper::simulateBreakup on a context: for every record with
+ * LADDS_PAIR_COLLISION (in order), both objects are marked deleted and the
+ * fragments of their collision appended (parentId = the record's idA; objects
+ * already broken up by an earlier record of the call are skipped).  Fragment
+ * ids start at *nextId, which is advanced (the reference passes its initial
+ * maximum id to every breakup).  Seed of record i: seed + i. */
+int ladds_gpu_breakup(ladds_gpu_ctx *ctx, const ladds_pair *records, size_t n, const ladds_breakup_config *cfg,
+                      uint64_t seed, uint64_t *nextId, size_t *nBreakups, size_t *nFragments);
+
 /* ---- conjunction record output (host functions) ----
  * The reference writes conjunctions as CSV (io/ConjuctionLogger.cpp:13-47:
  * header "Iteration,P1,P2,SquaredDistance", one line per pair with the

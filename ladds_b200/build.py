@@ -56,7 +56,7 @@ def build_gpu(force: bool = False, verbose: bool = False, ptxas_info: bool = Fal
         return GPU_LIB
     cmd = [nvcc(), *NVCC_ARCH, *NVCC_FLAGS, "-shared", "-o", GPU_LIB,
            os.path.join(CSRC, "ladds_gpu.cu"), os.path.join(CSRC, "population.cpp"),
-           os.path.join(CSRC, "records_io.cpp"), "-lgomp"]
+           os.path.join(CSRC, "records_io.cpp"), os.path.join(CSRC, "breakup.cpp"), "-lgomp"]
     if ptxas_info:
         cmd[1:1] = ["-Xptxas", "-v"]
     if verbose:

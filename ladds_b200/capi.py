@@ -84,8 +84,18 @@ EXPORTED = [
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
-    "ladds_records_write_csv", "ladds_gpu_checked_insert",
+    "ladds_records_write_csv", "ladds_gpu_checked_insert", "ladds_gpu_get_objects", "ladds_breakup_collision",
+    "ladds_gpu_breakup",
 ]
+
+STATE_RECORD_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("aom", "<f8"),
+                               ("bcInv", "<f8"), ("id", "<u8"), ("parentId", "<u8"), ("activity", "<i4"),
+                               ("deleted", "<u4")])
+assert STATE_RECORD_DTYPE.itemsize == 96
+
+
+class BreakupConfig(C.Structure):
+    _fields_ = [("minLc", C.c_double), ("enforceMassConservation", C.c_int32), ("coefficientOfDrag", C.c_double)]
 
 COLLISION_INFO_DTYPE = np.dtype([("idA", "<u4"), ("idB", "<u4"), ("distanceSquared", "<f4")])
 assert COLLISION_INFO_DTYPE.itemsize == 12
@@ -156,6 +166,11 @@ def lib():
     L.ladds_gpu_adjoint_forward.argtypes = [vp, vp, sz, i, i, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_backward.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
     L.ladds_gpu_adjoint_make_pairs.argtypes = [vp, C.c_uint64, sz, i, vp, vp]
+    L.ladds_gpu_get_objects.argtypes = [vp, vp, sz, vp]
+    L.ladds_breakup_collision.argtypes = [C.POINTER(BreakupConfig), C.c_uint64, vp, vp, vp, C.c_uint64,
+                                          C.POINTER(C.c_uint64), sz, C.POINTER(sz)] + [vp] * 12
+    L.ladds_gpu_breakup.argtypes = [vp, vp, sz, C.POINTER(BreakupConfig), C.c_uint64, C.POINTER(C.c_uint64),
+                                    C.POINTER(sz), C.POINTER(sz)]
     L.ladds_gpu_checked_insert.argtypes = [vp, sz] + [vp] * 12 + [C.c_double, vp, C.POINTER(sz)]
     L.ladds_records_pack.argtypes = [vp, sz, C.c_uint32, vp, sz, C.POINTER(sz)]
     L.ladds_records_write_csv.argtypes = [C.c_char_p, i, vp, sz, C.c_uint32]
@@ -402,6 +417,23 @@ class Context:
             self._check(rc)
             return out[: n.value].copy()
 
+    def get_objects(self, slots) -> np.ndarray:
+        """State records (STATE_RECORD_DTYPE) of the objects with the given slots."""
+        slots = np.ascontiguousarray(slots, dtype=np.uint32)
+        out = np.zeros(max(len(slots), 1), dtype=STATE_RECORD_DTYPE)
+        self._check(self._L.ladds_gpu_get_objects(self._h, _p(slots), len(slots), _p(out)))
+        return out[: len(slots)]
+
+    def breakup(self, records: np.ndarray, cfg: "BreakupConfig", seed: int, next_id: int):
+        """BreakupWrapper::simulateBreakup for the collision records; returns
+        (breakups, fragments, next free id)."""
+        records = np.ascontiguousarray(records, dtype=PAIR_DTYPE)
+        nid = C.c_uint64(next_id)
+        nb, nf = C.c_size_t(), C.c_size_t()
+        self._check(self._L.ladds_gpu_breakup(self._h, _p(records), len(records), C.byref(cfg), seed,
+                                              C.byref(nid), C.byref(nb), C.byref(nf)))
+        return nb.value, nf.value, nid.value
+
     def checked_insert(self, pop: dict, constellation_cutoff: float) -> np.ndarray:
         """Simulation::checkedInsert: appends the satellites of `pop` that have no
         particle within the cutoff; returns the delayed flags (1 = not inserted)."""
@@ -477,3 +509,23 @@ def write_records_csv(path: str, records: np.ndarray, flag_mask: int, append: bo
     rc = lib().ladds_records_write_csv(path.encode(), 1 if append else 0, _p(records), len(records), flag_mask)
     if rc:
         raise LaddsError(rc, f"ladds_records_write_csv({path}) failed")
+
+
+def breakup_collision(cfg: BreakupConfig, seed: int, a: np.ndarray, b: np.ndarray, point, parent_id: int,
+                      next_id: int, cap: int = 1 << 16):
+    """Fragments of one collision (host NASA-breakup restatement): (population dict, next free id)."""
+    a = np.ascontiguousarray(a, dtype=STATE_RECORD_DTYPE)
+    b = np.ascontiguousarray(b, dtype=STATE_RECORD_DTYPE)
+    pt = np.ascontiguousarray(point, dtype=np.float64)
+    while True:
+        pop = empty_population(cap)
+        nid = C.c_uint64(next_id)
+        got = C.c_size_t()
+        rc = lib().ladds_breakup_collision(C.byref(cfg), seed, _p(a), _p(b), _p(pt), parent_id, C.byref(nid), cap,
+                                           C.byref(got), *[_p(pop[k]) for k in POP_FIELDS])
+        if rc == ERR_CAPACITY:
+            cap = got.value
+            continue
+        if rc:
+            raise LaddsError(rc, "ladds_breakup_collision failed")
+        return {k: v[: got.value].copy() for k, v in pop.items()}, nid.value

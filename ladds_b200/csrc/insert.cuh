@@ -58,4 +58,44 @@ __global__ void k_insert_blocked(DevState s, int n, const double *__restrict__ n
   if (lane == 0) blocked[w] = hit ? 1 : 0;
 }
 
+// pos[q] = position in the state arrays of wanted slot q (wanted sorted ascending)
+__global__ void k_find_slots(const uint32_t *__restrict__ tags, int n, const uint32_t *__restrict__ wanted, int m,
+                             int32_t *__restrict__ pos) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t slot = tagSlot(tags[j]);
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (wanted[mid] < slot)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < m && wanted[lo] == slot) pos[lo] = j;
+}
+
+__global__ void k_gather_records(DevState s, const int32_t *__restrict__ pos, int m,
+                                 ladds_state_record *__restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const int32_t j = pos[q];
+  if (j < 0) return;
+  ladds_state_record r;
+  r.r[0] = s.x[j];
+  r.r[1] = s.y[j];
+  r.r[2] = s.z[j];
+  r.v[0] = s.vx[j];
+  r.v[1] = s.vy[j];
+  r.v[2] = s.vz[j];
+  r.radius = s.radius[j];
+  r.aom = s.aom[j];
+  r.bcInv = s.bc[j];
+  r.id = s.id[j];
+  r.parentId = s.parent[j];
+  r.activity = tagAct(s.tag[j]);
+  r.deleted = tagDummy(s.tag[j]) ? 1u : 0u;
+  out[q] = r;
+}
+
 }  // namespace ladds

@@ -965,6 +965,49 @@ int ladds_gpu_checked_insert(ladds_gpu_ctx *c, size_t n, const double *x, const 
   return rc;
 }
 
+int ladds_gpu_get_objects(ladds_gpu_ctx *c, const uint32_t *slots, size_t m, ladds_state_record *out) {
+  if (!c || (m && (!slots || !out))) return fail(c, LADDS_ERR_INVALID_ARG, "get_objects: bad argument");
+  if (!m) return LADDS_OK;
+  std::vector<uint32_t> want(slots, slots + m);
+  std::sort(want.begin(), want.end());
+  want.erase(std::unique(want.begin(), want.end()), want.end());
+  const int mu = (int)want.size();
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  CK(cudaSetDevice(c->dev));
+  uint32_t *dWant = nullptr;
+  int32_t *dPos = nullptr;
+  ladds_state_record *dRec = nullptr;
+  if (cudaMalloc(&dWant, mu * sizeof(uint32_t)) != cudaSuccess || cudaMalloc(&dPos, mu * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&dRec, mu * sizeof(ladds_state_record)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dWant);
+    cudaFree(dPos);
+    return fail(c, LADDS_ERR_ALLOC, "get_objects: staging allocation failed");
+  }
+  std::vector<int32_t> pos(mu, -1);
+  std::vector<ladds_state_record> rec(mu);
+  cudaError_t e = cudaMemcpyAsync(dWant, want.data(), mu * sizeof(uint32_t), cudaMemcpyHostToDevice, c->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dPos, 0xff, mu * sizeof(int32_t), c->st);
+  if (e == cudaSuccess && c->n)
+    k_find_slots<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.tag, (int)c->n, dWant, mu, dPos);
+  if (e == cudaSuccess) k_gather_records<<<blocksFor((size_t)mu, 128), 128, 0, c->st>>>(c->cur, dPos, mu, dRec);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pos.data(), dPos, mu * sizeof(int32_t), cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rec.data(), dRec, mu * sizeof(ladds_state_record), cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(dWant);
+  cudaFree(dPos);
+  cudaFree(dRec);
+  if (e != cudaSuccess) return fail(c, LADDS_ERR_CUDA, std::string("get_objects: ") + cudaGetErrorString(e));
+  for (size_t q = 0; q < m; ++q) {
+    const size_t k = std::lower_bound(want.begin(), want.end(), slots[q]) - want.begin();
+    if (pos[k] < 0) return fail(c, LADDS_ERR_INVALID_ARG, "get_objects: no object with slot " + std::to_string(slots[q]));
+    out[q] = rec[k];
+  }
+  return LADDS_OK;
+}
+
 int ladds_gpu_download(ladds_gpu_ctx *c, size_t cap, size_t *nOut, double *x, double *y, double *z, double *vx,
                        double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
                        uint64_t *parentId, int8_t *activity) {
