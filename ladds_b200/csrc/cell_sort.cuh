@@ -275,50 +275,55 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_small(
 // then 256 slots, 256 sources and 256 cell indices.
 constexpr int kRowCountMaxNx = 1023;
 constexpr int kRowSortThreads = 128;
-__host__ __device__ __forceinline__ uint32_t rowCountWords(uint32_t nx) { return (nx + 32u) & ~31u; }
+// counters of a row: nx + 1 rounded up to 32 x a power of two, so that each lane
+// owns a power-of-two run of them in the scan
+__host__ __device__ __forceinline__ uint32_t rowCountShift(uint32_t nx) {
+  uint32_t sh = 0;
+  while ((32u << sh) < nx + 1u) ++sh;
+  return sh;
+}
+__host__ __device__ __forceinline__ uint32_t rowCountWords(uint32_t nx) { return 32u << rowCountShift(nx); }
+// the counters are stored with one pad word after every run (index c + c / run),
+// so the lanes' runs start in different banks
+__host__ __device__ __forceinline__ uint32_t rowCountStored(uint32_t nx) {
+  return rowCountWords(nx) + 32u;
+}
+// per warp: counters, then 256 entries of (ix | arrival << 16), slot and source
+// in load order, then 256 slots, sources and cell indices in cell order
+__host__ __device__ __forceinline__ uint32_t rowSortWarpWords(uint32_t nx) {
+  return rowCountStored(nx) + 256u * 5u + 128u;
+}
 __host__ __device__ __forceinline__ size_t rowSortSmem(uint32_t nx) {
-  return (size_t)(kRowSortThreads / 32) * (rowCountWords(nx) * 4u + 256u * 10u);
+  return (size_t)(kRowSortThreads / 32) * rowSortWarpWords(nx) * 4u;
 }
 
-__global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
-    const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
-    const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
-    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff,
-    DenseBin dense) {
-  extern __shared__ uint32_t smemRows[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t H = rowCountWords(nx), per = H / 32u;
-  uint32_t *hist = smemRows + (size_t)warp * (H + 256u * 2u + 128u);
-  uint32_t *tSlot = hist + H, *tSrc = tSlot + 256;
-  uint16_t *tIx = reinterpret_cast<uint16_t *>(tSrc + 256);
-  const uint32_t pitch = cellOffPitch(nx);
-  const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t r = warpId; r < nRows; r += nWarps) {
-    const uint32_t s0 = rowStart[r], L = rowStart[r + 1] - s0;
-    if (L == 0) continue;
-    if (L > 256u) {
-      if (lane == 0) longRows[atomicAdd(longCount, 1u)] = r;
-      continue;
-    }
-    for (uint32_t c = lane; c < H; c += 32) hist[c] = 0u;
+// one row of <= 256 objects by one warp (see k_bucket_sort_rows); element
+// `lane` of the row is passed in (firstRec, firstSrc)
+__device__ __forceinline__ void sortOneRow(uint32_t r, uint32_t s0, uint32_t L, unsigned long long firstRec,
+                                           uint32_t firstSrc, int lane, uint32_t nx, uint32_t H, uint32_t sh,
+                                           uint32_t pitch, const unsigned long long *__restrict__ rec,
+                                           const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys,
+                                           uint32_t *__restrict__ perm, uint16_t *__restrict__ cellOff,
+                                           const DenseBin &dense, uint32_t *hist, uint32_t *inIxArr,
+                                           uint32_t *inSlot, uint32_t *inSrc, uint32_t *tSlot, uint32_t *tSrc,
+                                           uint16_t *tIx) {
+    const uint32_t per = 1u << sh;
+    auto at = [sh](uint32_t c) { return c + (c >> sh); };  // padded counter index
+    for (uint32_t c = lane; c < H + 32u; c += 32) hist[c] = 0u;
     __syncwarp();
-    uint32_t eIx[8], eSlot[8], eSrc[8], eArr[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const uint32_t e = (uint32_t)(q * 32 + lane);
-      if (e < L) {
-        const unsigned long long v = rec[s0 + e];
-        eIx[q] = (uint32_t)(v >> 32);
-        eSlot[q] = (uint32_t)v;
-        eSrc[q] = src[s0 + e];
-        eArr[q] = atomicAdd(&hist[eIx[q]], 1u);
-      }
+    // histogram of the cell indices; each object's arrival in its cell
+    for (uint32_t e = lane; e < L; e += 32) {
+      const unsigned long long v = e < 32u ? firstRec : rec[s0 + e];
+      const uint32_t ix = (uint32_t)(v >> 32);
+      inIxArr[e] = ix | (atomicAdd(&hist[at(ix)], 1u) << 16);
+      inSlot[e] = (uint32_t)v;
+      inSrc[e] = e < 32u ? firstSrc : src[s0 + e];
     }
     __syncwarp();
     // exclusive scan of the counts: lane l owns counters [l * per, (l + 1) * per)
+    uint32_t *run0 = hist + lane * (per + 1u);
     uint32_t sum = 0;
-    for (uint32_t i = 0; i < per; ++i) sum += hist[lane * per + i];
+    for (uint32_t i = 0; i < per; ++i) sum += run0[i];
     uint32_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -328,29 +333,26 @@ __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
     uint32_t run = incl - sum;
     const bool listDense = cellOff && dense.cells && L >= dense.minCount;
     for (uint32_t i = 0; i < per; ++i) {
-      const uint32_t cc = lane * per + i, c = hist[cc];
-      hist[cc] = run;
+      const uint32_t c = run0[i];
+      run0[i] = run;
       run += c;
-      if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + cc);  // cc < nx: counts past nx are 0
+      if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * per + i);  // counts past nx are 0
     }
     __syncwarp();
     if (cellOff) {
       uint16_t *t = cellOff + (size_t)r * pitch;
-      for (uint32_t c = lane; c <= nx; c += 32) t[c] = (uint16_t)hist[c];
+      for (uint32_t c = lane; c <= nx; c += 32) t[c] = (uint16_t)hist[at(c)];
     }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const uint32_t e = (uint32_t)(q * 32 + lane);
-      if (e < L) {
-        const uint32_t p = hist[eIx[q]] + eArr[q];
-        tSlot[p] = eSlot[q];
-        tSrc[p] = eSrc[q];
-        tIx[p] = (uint16_t)eIx[q];
-      }
+    for (uint32_t e = lane; e < L; e += 32) {  // place in cell order (arrival order inside a cell)
+      const uint32_t ia = inIxArr[e], ix = ia & 0xffffu;
+      const uint32_t p = hist[at(ix)] + (ia >> 16);
+      tSlot[p] = inSlot[e];
+      tSrc[p] = inSrc[e];
+      tIx[p] = (uint16_t)ix;
     }
     __syncwarp();
-    for (uint32_t p = lane; p < L; p += 32) {
-      const uint32_t ix = tIx[p], c0 = hist[ix], c1 = hist[ix + 1], sl = tSlot[p];
+    for (uint32_t p = lane; p < L; p += 32) {  // rank by slot inside the cell
+      const uint32_t ix = tIx[p], c0 = hist[at(ix)], c1 = hist[at(ix + 1)], sl = tSlot[p];
       uint32_t rank = 0;
       for (uint32_t q = c0; q < c1; ++q) rank += tSlot[q] < sl ? 1u : 0u;
       const uint32_t out = s0 + c0 + rank;
@@ -358,8 +360,73 @@ __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
       perm[out] = tSrc[p];
     }
     __syncwarp();
+}
+
+__global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
+    const uint32_t *__restrict__ rowStart, uint32_t nRows, uint32_t nx, const unsigned long long *__restrict__ rec,
+    const uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
+    uint32_t *__restrict__ longRows, uint32_t *__restrict__ longCount, uint16_t *__restrict__ cellOff,
+    DenseBin dense) {
+  extern __shared__ uint32_t smemRows[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t sh = rowCountShift(nx), H = rowCountWords(nx);
+  uint32_t *hist = smemRows + (size_t)warp * rowSortWarpWords(nx);
+  uint32_t *inIxArr = hist + rowCountStored(nx), *inSlot = inIxArr + 256, *inSrc = inSlot + 256;
+  uint32_t *tSlot = inSrc + 256, *tSrc = tSlot + 256;
+  uint16_t *tIx = reinterpret_cast<uint16_t *>(tSrc + 256);
+  const uint32_t pitch = cellOffPitch(nx);
+  const uint32_t warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
+  // software pipeline over the warp's rows: the row starts two rows ahead and
+  // the first 32 records one row ahead are in flight while a row is sorted
+  uint32_t r = warpId, s0 = 0, L = 0, firstSrc = 0;
+  unsigned long long firstRec = 0;
+  if (r < nRows) {
+    s0 = rowStart[r];
+    L = rowStart[r + 1] - s0;
+    if ((uint32_t)lane < L && L <= 256u) {
+      firstRec = rec[s0 + lane];
+      firstSrc = src[s0 + lane];
+    }
+  }
+  uint32_t rN = r + nWarps, sN = 0, eN = 0;
+  if (rN < nRows) {
+    sN = rowStart[rN];
+    eN = rowStart[rN + 1];
+  }
+  for (; r < nRows; r = rN, rN += nWarps) {
+    const uint32_t lN = eN - sN;
+    unsigned long long nextRec = 0;
+    uint32_t nextSrc = 0;
+    if (rN < nRows && (uint32_t)lane < lN && lN <= 256u) {
+      nextRec = rec[sN + lane];
+      nextSrc = src[sN + lane];
+    }
+    const uint32_t rNN = rN + nWarps;
+    uint32_t sNN = 0, eNN = 0;
+    if (rNN < nRows) {
+      sNN = rowStart[rNN];
+      eNN = rowStart[rNN + 1];
+    }
+    const uint32_t rowS0 = s0, rowL = L;
+    const unsigned long long rowFirstRec = firstRec;
+    const uint32_t rowFirstSrc = firstSrc;
+    s0 = sN;
+    L = lN;
+    firstRec = nextRec;
+    firstSrc = nextSrc;
+    sN = sNN;
+    eN = eNN;
+    if (rowL == 0) continue;
+    if (rowL > 256u) {
+      if (lane == 0) longRows[atomicAdd(longCount, 1u)] = r;
+      continue;
+    }
+    sortOneRow(r, rowS0, rowL, rowFirstRec, rowFirstSrc, lane, nx, H, sh, pitch, rec, src, sortedKeys, perm,
+               cellOff, dense, hist, inIxArr, inSlot, inSrc, tSlot, tSrc, tIx);
   }
 }
+
 
 __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
     const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,

@@ -484,7 +484,8 @@ void enqueueSort(ladds_gpu_ctx *c) {
   PhaseScope ps(c, kPhRowsort, c->st, 2);
   const DenseBin dense = denseBin(c);
   if (nx <= (uint32_t)kRowCountMaxNx) {  // counting sort inside the rows
-    const int rowBlocks = std::min(blocksFor((size_t)nRows * 32, kRowSortThreads), 32 * c->evalBlocks);
+    // one resident wave (8 CTAs of 4 warps per SM by shared memory); each warp pipelines its rows
+    const int rowBlocks = std::min(blocksFor((size_t)nRows * 32, kRowSortThreads), 2 * c->evalBlocks);
     k_bucket_sort_rows<<<rowBlocks, kRowSortThreads, rowSortSmem(nx), c->st>>>(
         c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff,
         dense);
