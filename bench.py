@@ -143,12 +143,12 @@ def algorithmic_units(n):
         "bucket": {"bytes": n * (4 + 8 + 12)},
         # row sort: record + source in (12), sorted key + slot out (8)
         "rowsort": {"bytes": n * (12 + 8)},
-        # gather 92 B + perm 4 into cell order; write 92 B SoA + 96 B packed + 16 B binary32 copy
-        "permute": {"bytes": n * (92 + 4 + 92 + 96 + 16)},
+        # gather 92 B + perm 4 into cell order; write 92 B SoA + 32 B binary32 position / velocity copies
+        "permute": {"bytes": n * (92 + 4 + 92 + 32)},
         # own key, tag, pos4, posf (56 B) + ~1 candidate write (12 B)
         "candidates": {"bytes": n * (56 + 12)},
-        # packed records of both objects of each candidate, once from DRAM (80 B per object)
-        "evaluate": {"bytes": n * 80},
+        # binary32 position + velocity of both objects of each candidate (64 B, ~1.5 candidates per object)
+        "evaluate": {"bytes": n * 96},
     }
 
 

@@ -28,14 +28,16 @@ __device__ __forceinline__ float4 floatPosition(double x, double y, double z) {
   return make_float4((float)x, (float)y, (float)z, (float)(m * 0x1p-22) + 1e-12f);
 }
 
-// Packed copies of the cell-ordered population read by the pair scan: one
-// 32-byte sector per load (positions + radius, velocities + id, parent + tag).
+// What the pair scan reads of the cell-ordered population: binary32 copies
+// (positions with their rounding bound, velocities with the radius rounded up)
+// in cell order, and, for the few pairs that reach the binary64 functor, the
+// state as it was before the gather (src, indexed through perm) -- the next
+// propagation, which runs beside the scan, writes only the gathered copy.
 struct ScanPack {
-  double4 *pos4;      // x, y, z, radius
-  double4 *vel4;      // vx, vy, vz, id (bit pattern)
-  ulonglong2 *meta;   // parentId, tag
-  float4 *posf;       // binary32 x, y, z + rounding bound
-  float4 *velf;       // binary32 vx, vy, vz + radius rounded up
+  float4 *posf;          // binary32 x, y, z + rounding bound
+  float4 *velf;          // binary32 vx, vy, vz + radius rounded up
+  DevState src;          // state before the gather
+  const uint32_t *perm;  // cell-order position -> index in src
 };
 
 __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n, ScanPack pk,
@@ -64,9 +66,6 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   dst.id[j] = id;
   dst.parent[j] = parent;
   dst.tag[j] = tag;
-  pk.pos4[j] = make_double4(x, y, z, radius);
-  pk.vel4[j] = make_double4(vx, vy, vz, __longlong_as_double((long long)id));
-  pk.meta[j] = make_ulonglong2(parent, tag);
   pk.posf[j] = floatPosition(x, y, z);
   pk.velf[j] = make_float4((float)vx, (float)vy, (float)vz, __double2float_ru(radius));
 }
@@ -113,18 +112,17 @@ struct Obj {
 };
 
 __device__ __forceinline__ void loadObjPacked(const ScanPack &pk, uint32_t k, Obj &o) {
-  const double4 a = pk.pos4[k], b = pk.vel4[k];
-  const ulonglong2 m = pk.meta[k];
-  o.r[0] = a.x;
-  o.r[1] = a.y;
-  o.r[2] = a.z;
-  o.radius = a.w;
-  o.v[0] = b.x;
-  o.v[1] = b.y;
-  o.v[2] = b.z;
-  o.id = (uint64_t)__double_as_longlong(b.w);
-  o.parent = m.x;
-  o.tag = (uint32_t)m.y;
+  const uint32_t p = pk.perm[k];
+  o.r[0] = pk.src.x[p];
+  o.r[1] = pk.src.y[p];
+  o.r[2] = pk.src.z[p];
+  o.radius = pk.src.radius[p];
+  o.v[0] = pk.src.vx[p];
+  o.v[1] = pk.src.vy[p];
+  o.v[2] = pk.src.vz[p];
+  o.id = pk.src.id[p];
+  o.parent = pk.src.parent[p];
+  o.tag = pk.src.tag[p];
 }
 
 __device__ __forceinline__ void loadObj(const DevState &s, int k, Obj &o) {

@@ -83,13 +83,10 @@ struct ladds_gpu_ctx {
   uint16_t *cellOff = nullptr;            // per row: offset of every cell inside the row (cellOffPitch entries)
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
   float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
-  double4 *vel4 = nullptr;                // vx, vy, vz, id of the cell order
   float4 *velf = nullptr;                 // binary32 velocities + radius of the cell order
-  ulonglong2 *meta = nullptr;             // parentId, tag of the cell order
   uint32_t *rowStart = nullptr;
   uint32_t nRows = 0;
   uint32_t *scratchA = nullptr, *scratchB = nullptr, *scratchC = nullptr, *blockSums = nullptr;
-  double4 *pos4 = nullptr;  // packed positions in cell order (pair-scan candidate test)
   ladds_pair *dPairs = nullptr;
   size_t pairCap = 0;
   unsigned long long *dCount = nullptr;
@@ -189,14 +186,11 @@ void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->alt);
   freeState(c->snap);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums, c->pos4, c->posf, c->sortRec, c->scanWs, c->vel4, c->meta, c->velf};
+                  c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  c->pos4 = nullptr;
   c->posf = nullptr;
-  c->vel4 = nullptr;
   c->velf = nullptr;
-  c->meta = nullptr;
   c->sortRec = nullptr;
   c->scanWs = nullptr;
   c->keys0 = c->keys1 = c->vals0 = c->vals1 = nullptr;
@@ -244,11 +238,8 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   // block sums of the three-level exclusive scans (objects or rows, whichever is longer)
   const size_t scanLen = std::max(newCap + 1, (size_t)c->nRows + 1);
   const size_t wsWords = 4 * (scanLen / kScanBlock + 2) + 4 * kScanBlock;
-  if (cudaMalloc(&c->pos4, newCap * sizeof(double4)) != cudaSuccess ||
-      cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
-      cudaMalloc(&c->vel4, newCap * sizeof(double4)) != cudaSuccess ||
+  if (cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&c->velf, newCap * sizeof(float4)) != cudaSuccess ||
-      cudaMalloc(&c->meta, newCap * sizeof(ulonglong2)) != cudaSuccess ||
       cudaMalloc(&c->sortRec, newCap * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->blockSums, (scanBlocks + 1) * sizeof(uint32_t)) != cudaSuccess) {
@@ -500,7 +491,8 @@ void enqueueSort(ladds_gpu_ctx *c) {
   c->perm = c->vals1;
 }
 
-inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->pos4, c->vel4, c->meta, c->posf, c->velf}; }
+// after the gather (enqueueCells) alt holds the state as the scan sees it, perm maps into it
+inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->posf, c->velf, c->alt, c->perm}; }
 
 // gathers the state into cell order (so that the next propagation, key pass and
 // gather read nearly sequentially: objects move about one cell per step) and
@@ -525,11 +517,11 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
     cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), s);
     k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
-        c->cur.tag, c->pos4, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
+        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
         sc.nearRel, cutF, dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, c->dCand, c->dCandCount,
         (unsigned long long)c->candCap);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
-      k_pair_tiles<<<4 * c->evalBlocks, kScanCta, 0, s>>>(dense.cells, dense.count, dense.cap, c->cur.tag, c->pos4,
+      k_pair_tiles<<<4 * c->evalBlocks, kScanCta, 0, s>>>(dense.cells, dense.count, dense.cap, c->cur.tag,
                                                       c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
                                                       sc.cutoffSq, sc.nearRel, cutF, c->dCand, c->dCandCount,
                                                       (unsigned long long)c->candCap);

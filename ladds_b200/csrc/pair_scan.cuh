@@ -129,7 +129,6 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
 // its near band accepts passes the binary32 test.  The loops over the
 // neighbour rows are warp-uniform; inactive lanes contribute empty windows.
 __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__restrict__ tags,
-                                                              const double4 *__restrict__ pos4,
                                                               const float4 *__restrict__ posf, int n,
                                                               const uint32_t *__restrict__ skeys,
                                                               const uint32_t *__restrict__ rowStart,
@@ -214,7 +213,6 @@ __device__ __forceinline__ int halfShellRowOf(int q, int R, int &dz, int &dy) {
 __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restrict__ denseCells,
                                                          const uint32_t *__restrict__ denseCount, uint32_t denseCap,
                                                          const uint32_t *__restrict__ tags,
-                                                         const double4 *__restrict__ pos4,
                                                          const float4 *__restrict__ posf,
                                                          const uint32_t *__restrict__ skeys,
                                                          const uint32_t *__restrict__ rowStart,
