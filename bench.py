@@ -145,10 +145,11 @@ def algorithmic_units(n):
         "rowsort": {"bytes": n * (12 + 8)},
         # gather 92 B + perm 4 into cell order; write 92 B SoA + 32 B binary32 position / velocity copies
         "permute": {"bytes": n * (92 + 4 + 92 + 32)},
-        # own key, tag, pos4, posf (56 B) + ~1 candidate write (12 B)
-        "candidates": {"bytes": n * (56 + 12)},
-        # binary32 position + velocity of both objects of each candidate (64 B, ~1.5 candidates per object)
-        "evaluate": {"bytes": n * 96},
+        # own key, tag, posf (24 B) + the closest-approach screen of the pre-filtered pairs: binary32
+        # position + velocity of both objects (64 B, ~1.5 pairs per object)
+        "candidates": {"bytes": n * (24 + 96)},
+        # FP64 records of the few screened pairs (a few per thousand objects): no per-object traffic
+        "evaluate": {"bytes": 0},
     }
 
 

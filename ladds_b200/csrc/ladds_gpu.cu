@@ -91,8 +91,8 @@ struct ladds_gpu_ctx {
   size_t pairCap = 0;
   unsigned long long *dCount = nullptr;
   uint2 *dCand = nullptr;  // candidate pairs (sorted indices) of the pair scan
-  size_t candCap = 0;
-  unsigned long long *dCandCount = nullptr;  // candidates of the current scan
+  size_t candCap = 0;  // entries of each of the two candidate lists
+  unsigned long long *dCandCount = nullptr;  // lengths of the candidate lists of the current scan
   unsigned long long *dCandNeed = nullptr;   // largest candidate count of the call
   unsigned *dStatus = nullptr;
   EphEntry *dEph = nullptr;
@@ -114,6 +114,12 @@ struct ladds_gpu_ctx {
   int chunkSteps = kMaxEphSteps;  // iterations per ephemeris chunk / captured graph (autotuned)
   uint32_t *denseCells = nullptr, *denseCount = nullptr;  // dense bin of the pair scan (cells >= kDenseCell)
   uint32_t denseCap = 0;
+  // second set of the sort results: the sort of a step writes one set while the
+  // pair scan of the previous step still reads the other
+  uint32_t *rowStartB = nullptr, *keys1B = nullptr, *vals1B = nullptr, *denseCellsB = nullptr,
+           *denseCountB = nullptr;
+  uint16_t *cellOffB = nullptr;
+  int sortParity = 0;
   struct Adjoint {          // buffers of the adjoint pair batch (ladds_gpu_adjoint_*)
     size_t nPairs = 0;
     int steps = 0, ck = 0;
@@ -186,14 +192,14 @@ void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->alt);
   freeState(c->snap);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf};
+                  c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf, c->keys1B, c->vals1B};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c->posf = nullptr;
   c->velf = nullptr;
   c->sortRec = nullptr;
   c->scanWs = nullptr;
-  c->keys0 = c->keys1 = c->vals0 = c->vals1 = nullptr;
+  c->keys0 = c->keys1 = c->vals0 = c->vals1 = c->keys1B = c->vals1B = nullptr;
   c->scratchA = c->scratchB = c->scratchC = c->blockSums = nullptr;
   c->sortedKeys = c->perm = nullptr;
   c->cap = 0;
@@ -228,7 +234,8 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   c->snap = nsnap;
   c->homeX = ncur.x;
   const size_t scanBlocks = (newCap + 1 + kScanBlock - 1) / kScanBlock;
-  uint32_t **u[] = {&c->keys0, &c->keys1, &c->vals0, &c->vals1, &c->scratchA, &c->scratchB, &c->scratchC};
+  uint32_t **u[] = {&c->keys0,    &c->keys1,    &c->vals0,  &c->vals1, &c->scratchA,
+                    &c->scratchB, &c->scratchC, &c->keys1B, &c->vals1B};
   for (uint32_t **p : u) {
     if (cudaMalloc(p, (newCap + 1) * sizeof(uint32_t)) != cudaSuccess) {
       cudaGetLastError();
@@ -247,18 +254,23 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
     return fail(c, LADDS_ERR_ALLOC, "device allocation failed (cell-order buffers)");
   }
   if (c->denseCells) cudaFree(c->denseCells);
+  if (c->denseCellsB) cudaFree(c->denseCellsB);
+  c->denseCells = c->denseCellsB = nullptr;
   c->denseCap = (uint32_t)(newCap / kDenseCell + 1);
-  if (cudaMalloc(&c->denseCells, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
+  if (cudaMalloc(&c->denseCells, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->denseCellsB, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
-    c->denseCells = nullptr;
+    if (c->denseCells) cudaFree(c->denseCells);
+    c->denseCells = c->denseCellsB = nullptr;
     c->denseCap = 0;
     return fail(c, LADDS_ERR_ALLOC, "device allocation failed (dense-cell list)");
   }
   c->cap = newCap;
   c->orderValid = false;
   dropGraphs(c);
-  // about 1.5 gated candidates per object at LEO densities; the buffer grows on overflow
-  return ensureCandCapacity(c, std::max<size_t>(2 * newCap, (size_t)1 << 16));
+  // candidates that pass the closest-approach screen: a few per thousand objects at LEO
+  // densities; the buffer grows on overflow
+  return ensureCandCapacity(c, std::max<size_t>(newCap / 8, (size_t)1 << 16));
 }
 
 int ensurePairCapacity(ladds_gpu_ctx *c, size_t need) {
@@ -279,8 +291,8 @@ int ensurePairCapacity(ladds_gpu_ctx *c, size_t need) {
 int ensureCandCapacity(ladds_gpu_ctx *c, size_t need) {
   if (need <= c->candCap) return LADDS_OK;
   size_t newCap = std::max<size_t>(need + need / 2, 1);
-  uint2 *p = nullptr;
-  if (cudaMalloc(&p, newCap * sizeof(uint2)) != cudaSuccess) {
+  uint2 *p = nullptr;  // the screened and the spilled list, newCap entries each
+  if (cudaMalloc(&p, 2 * newCap * sizeof(uint2)) != cudaSuccess) {
     cudaGetLastError();
     return fail(c, LADDS_ERR_ALLOC, "device allocation failed (candidate buffer)");
   }
@@ -457,11 +469,23 @@ DenseBin denseBin(const ladds_gpu_ctx *c) {
   return DenseBin{on ? c->denseCells : nullptr, c->denseCount, c->denseCap, kDenseCell};
 }
 
+// the sort writes the result set that the previous pair scan does not read
+void swapSortSets(ladds_gpu_ctx *c) {
+  std::swap(c->rowStart, c->rowStartB);
+  std::swap(c->keys1, c->keys1B);
+  std::swap(c->vals1, c->vals1B);
+  std::swap(c->cellOff, c->cellOffB);
+  std::swap(c->denseCells, c->denseCellsB);
+  std::swap(c->denseCount, c->denseCountB);
+  c->sortParity ^= 1;
+}
+
 // keys0 holds the keys of c->cur in current order, rowCounts their row counts
 // and scratchC their arrival indices (k_propagate<*, true> or k_cell_keys) ->
 // sortedKeys (keys1), perm (vals1) and the row-start table; order = sort by
 // (cell key, slot)
 void enqueueSort(ladds_gpu_ctx *c) {
+  swapSortSets(c);
   const int n = (int)c->n;
   const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
   {
@@ -515,21 +539,20 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
   const DenseBin dense = denseBin(c);
   {
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
-    cudaMemsetAsync(c->dCandCount, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
+    const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap};
     k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
-        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, sc.cutoffSq,
-        sc.nearRel, cutF, dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, c->dCand, c->dCandCount,
-        (unsigned long long)c->candCap);
+        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF,
+        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, out);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       k_pair_tiles<<<4 * c->evalBlocks, kScanCta, 0, s>>>(dense.cells, dense.count, dense.cap, c->cur.tag,
                                                       c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
-                                                      sc.cutoffSq, sc.nearRel, cutF, c->dCand, c->dCandCount,
-                                                      (unsigned long long)c->candCap);
+                                                      cutF, out);
   }
   PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
-  // one thread per possible candidate (the count is only known on the device)
-  const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), 32768));
+  // grid-stride over the screened candidates (their count is only known on the device; few per step)
+  const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), c->evalBlocks / 2));
   k_pair_eval<<<evalGrid, b, 0, s>>>(scanPack(c), c->dCand, c->dCandCount, (unsigned long long)c->candCap,
                                      c->dCandNeed, sc, iterPtr, iterOffset, c->dPairs, c->dCount,
                                      (unsigned long long)c->pairCap);
@@ -539,10 +562,12 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
 // `len` iterations starting at iteration itStart (len <= kMaxEphSteps): one
 // ephemeris kernel + one constant-memory copy for the whole chunk.  The pair
 // scan of iteration i (candidates + evaluation) runs on the second stream,
-// concurrently with the propagation of iteration i+1: the scan reads only the
-// packed cell-order copies, the cell tables and the tags, none of which the
-// propagation writes; the next sort / gather waits for the scan.  Records
-// carry the chunk's first iteration (stored by the ephemeris kernel) + i.
+// concurrently with the propagation and the sort of the next scanned
+// iteration: the scan reads the packed cell-order copies, the pre-gather state,
+// the tags and one set of sort results; the propagation writes none of them and
+// the sort writes the other set.  The next gather, which overwrites the packed
+// copies and the pre-gather state, waits for the scan.  Records carry the
+// chunk's first iteration (stored by the ephemeris kernel) + i.
 void enqueueChunk(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
   enqueueEphemeris(c, len);
   const bool overlap = !c->profiling;
@@ -551,11 +576,11 @@ void enqueueChunk(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
     const bool scan = ((itStart + i) % k) == 0 && c->n;
     enqueuePropagate(c, 1, scan, 3 * i);
     if (!scan) continue;
+    enqueueSort(c);
     if (pending) {
       cudaStreamWaitEvent(c->st, c->evScan, 0);
       pending = false;
     }
-    enqueueSort(c);
     enqueueCells(c);
     ScanConsts sc = c->sc;
     sc.dt = c->cfg.deltaT * (double)k;
@@ -577,7 +602,10 @@ void replaySwaps(ladds_gpu_ctx *c, int64_t itStart, int len, int k) {
   int scans = 0;
   for (int i = 0; i < len; ++i) scans += ((itStart + i) % k) == 0;
   if (!scans || !c->n) return;
-  if (scans % 2 == 1) std::swap(c->cur, c->alt);
+  if (scans % 2 == 1) {
+    std::swap(c->cur, c->alt);
+    swapSortSets(c);
+  }
   c->sortedKeys = c->keys1;
   c->perm = c->vals1;
 }
@@ -676,16 +704,17 @@ int buildGrid(ladds_gpu_ctx *c) {
 }
 
 void freeGridBuffers(ladds_gpu_ctx *c) {
-  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->cellOff};
+  void *ptrs[] = {c->rowStart, c->rowStartB, c->rowCounts, c->longRows, c->cellOff, c->cellOffB};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  c->rowStart = c->rowCounts = c->longRows = nullptr;
-  c->cellOff = nullptr;
+  c->rowStart = c->rowStartB = c->rowCounts = c->longRows = nullptr;
+  c->cellOff = c->cellOffB = nullptr;
 }
 
-// row tables of c->grid; the cell-offset table when it fits 1 GiB (250^3 cells: 31 MB)
+// row tables of c->grid; the two cell-offset tables when each fits 512 MiB (250^3 cells: 31 MB)
 int allocGridBuffers(ladds_gpu_ctx *c) {
   if (cudaMalloc(&c->rowStart, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->rowStartB, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->rowCounts, 2 * ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->longRows, ((size_t)c->nRows + 1) * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
@@ -693,9 +722,11 @@ int allocGridBuffers(ladds_gpu_ctx *c) {
     return fail(c, LADDS_ERR_ALLOC, "device allocation of the cell-row tables failed");
   }
   const size_t cellOffBytes = (size_t)c->nRows * cellOffPitch((uint32_t)c->grid.n[0]) * sizeof(uint16_t);
-  if (cellOffBytes <= ((size_t)1 << 30) && cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess) {
+  if (cellOffBytes <= ((size_t)1 << 29) && (cudaMalloc(&c->cellOff, cellOffBytes) != cudaSuccess ||
+                                               cudaMalloc(&c->cellOffB, cellOffBytes) != cudaSuccess)) {
     cudaGetLastError();
-    c->cellOff = nullptr;  // the scan then searches the sorted keys
+    if (c->cellOff) cudaFree(c->cellOff);
+    c->cellOff = c->cellOffB = nullptr;  // the scan then searches the sorted keys
   }
   return LADDS_OK;
 }
@@ -780,8 +811,9 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       allocGridBuffers(c) != LADDS_OK || cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->denseCount, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->denseCountB, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->dCount, sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&c->dCandCount, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dCandCount, 2 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dStatus, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
@@ -799,7 +831,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaEventCreate(&c->callEnd);
   cudaEventCreateWithFlags(&c->evCells, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
-  cudaMemset(c->dCandCount, 0, sizeof(unsigned long long));
+  cudaMemset(c->dCandCount, 0, 2 * sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);
@@ -823,9 +855,10 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   dropGraphs(c);
   freeBuffers(c);
-  void *ptrs[] = {c->rowStart, c->rowCounts, c->longRows, c->longCount, c->denseCount, c->denseCells, c->dCount,
+  freeGridBuffers(c);
+  void *ptrs[] = {c->longCount, c->denseCount, c->denseCells, c->denseCountB, c->denseCellsB, c->dCount,
                   c->dStatus, c->dEph,
-                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->cellOff, c->dObj,
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->dObj,
                   c->adj.st, c->adj.bc, c->adj.aom, c->adj.miss, c->adj.grad, c->adj.ckpt, c->adj.rec,
                   c->adj.off, c->adj.arg, c->adj.eph};
   for (void *p : ptrs)
@@ -1257,10 +1290,11 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       // between the timing events
       const DevState cur0 = c->cur, alt0 = c->alt;
       uint32_t *const sk0 = c->sortedKeys, *const pm0 = c->perm;
+      const int par0 = c->sortParity;
       for (int done = 0; done < iterations;) {
         const int len = std::min(iterations - done, c->chunkSteps);
-        const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
-                                         c->pairCap);
+        const int bufs = (c->cur.x == c->homeX ? 0 : 1) | 2 * c->sortParity;
+        const auto key = std::make_tuple(len, (int)((it0 + done) % k), bufs, c->n, c->pairCap);
         if (c->graphs.find(key) == c->graphs.end()) {
           CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
           enqueueChunk(c, it0 + done, len, k);
@@ -1278,14 +1312,15 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       }
       c->cur = cur0;
       c->alt = alt0;
+      if (c->sortParity != par0) swapSortSets(c);
       c->sortedKeys = sk0;
       c->perm = pm0;
       // pass 2: replay
       CK(cudaEventRecord(c->callStart, c->st));
       for (int done = 0; done < iterations;) {
         const int len = std::min(iterations - done, c->chunkSteps);
-        const auto key = std::make_tuple(len, (int)((it0 + done) % k), c->cur.x == c->homeX ? 0 : 1, c->n,
-                                         c->pairCap);
+        const int bufs = (c->cur.x == c->homeX ? 0 : 1) | 2 * c->sortParity;
+        const auto key = std::make_tuple(len, (int)((it0 + done) % k), bufs, c->n, c->pairCap);
         auto git = c->graphs.find(key);
         if (git == c->graphs.end()) return fail(c, LADDS_ERR_STATE, "graph cache inconsistent");
         replaySwaps(c, it0 + done, len, k);

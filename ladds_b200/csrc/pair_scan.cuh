@@ -9,13 +9,18 @@
 // binary search on the sorted keys.  A binary32 distance test with a margin
 // larger than its rounding error (and than the near band of the gate) keeps a
 // superset of the pairs within the cutoff.  Candidates are buffered per warp in
-// shared memory and appended with one global atomic per warp (no block
-// barriers).  Objects of cells with >= kDenseCell objects are sources of
-// k_pair_tiles instead (the occupancy bin of crowded cells).
+// shared memory (no block barriers).  At the end of the walk a warp screens its
+// buffer 32 pairs at a time with the binary32 closest-approach test mayRecord
+// and appends the few pairs that can yield a record to the screened list; a
+// buffer that fills up during the walk is appended unscreened to the second
+// list (keeping the screen out of the walk's registers).  Objects of cells with
+// >= kDenseCell objects are sources of k_pair_tiles instead (the occupancy bin
+// of crowded cells).
 //
-// Phase 2, k_pair_eval: one thread per candidate applies the exact binary64
-// cutoff gate d^2 <= cutoff^2 (CollisionFunctor.cpp:71-77, same rounding) and
-// the functor (CollisionFunctor.cpp:40-131), and appends the records.
+// Phase 2, k_pair_eval: one thread per listed candidate (unscreened ones are
+// screened first) applies the exact binary64 cutoff gate d^2 <= cutoff^2
+// (CollisionFunctor.cpp:71-77, same rounding) and the functor
+// (CollisionFunctor.cpp:40-131), and appends the records.
 #pragma once
 #include "cell_sort.cuh"
 #include "conjunction.cuh"
@@ -56,31 +61,71 @@ __device__ __forceinline__ bool prefilterPass(float4 mf, float4 q, float cutF) {
   return !(dx * dx + dy * dy + dz * dz > lim * lim * 1.000001f);
 }
 
+// Where the pre-filtered pairs of a scan go: the screen's constants and
+// binary32 copies, and the two global candidate lists -- screened pairs in
+// cand[0, half), unscreened spills of full warp buffers in cand[half, 2 half);
+// count[0] and count[1] are their lengths (which may exceed half: the caller
+// grows the lists and re-runs the scan).
+struct CandSink {
+  ScanConsts sc;
+  const float4 *posf, *velf;
+  uint2 *cand;
+  unsigned long long *count;
+  unsigned long long half;
+};
+
 // Per-warp candidate buffer in shared memory with its fill count n held in a
-// register (warp-uniform): appends are ballots, no atomics; a full buffer is
-// written out with one global atomic.  Every lane of the warp calls these.
-__device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, uint2 *__restrict__ cand,
-                                          unsigned long long *__restrict__ candCount, unsigned long long candCap) {
+// register (warp-uniform): appends are ballots, no atomics.  Every lane of the
+// warp calls these.
+//
+// A full buffer during the walk: appended unscreened with one global atomic.
+__device__ __forceinline__ void warpSpill(int lane, uint2 *buf, uint32_t &n, const CandSink &out) {
   __syncwarp();
   if (n) {
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(candCount, (unsigned long long)n);
+    if (lane == 0) base = atomicAdd(&out.count[1], (unsigned long long)n);
     base = __shfl_sync(0xffffffffu, base, 0);
     for (uint32_t i = (uint32_t)lane; i < n; i += 32u) {
       const unsigned long long pos = base + i;
-      if (pos < candCap) cand[pos] = buf[i];
+      if (pos < out.half) out.cand[out.half + pos] = buf[i];
     }
     __syncwarp();
   }
   n = 0;
 }
 
+// The buffer at the end of the walk: screened 32 pairs at a time (all four
+// loads of a lane in flight together); the survivors are appended with one
+// global atomic per round that has any.
+__device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, const CandSink &out) {
+  __syncwarp();
+  for (uint32_t b = 0; b < n; b += 32u) {
+    const uint32_t i = b + (uint32_t)lane;
+    uint2 p = make_uint2(0u, 0u);
+    bool keep = false;
+    if (i < n) {
+      p = buf[i];
+      keep = mayRecord(out.sc, __ldg(&out.posf[p.x]), __ldg(&out.velf[p.x]), __ldg(&out.posf[p.y]),
+                       __ldg(&out.velf[p.y]));
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+    if (mask) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&out.count[0], (unsigned long long)__popc(mask));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      const unsigned long long pos = base + (unsigned long long)__popc(mask & laneMaskLt());
+      if (keep && pos < out.half) out.cand[pos] = p;
+    }
+  }
+  __syncwarp();
+  n = 0;
+}
+
 __device__ __forceinline__ void warpAppend(bool pass, uint32_t j, uint32_t k, int lane, uint2 *buf, uint32_t &n,
-                                           uint2 *__restrict__ cand, unsigned long long *__restrict__ candCount,
-                                           unsigned long long candCap) {
+                                           const CandSink &out) {
   const uint32_t mask = __ballot_sync(0xffffffffu, pass);
   if (!mask) return;
-  if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) warpFlush(lane, buf, n, cand, candCount, candCap);
+  if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) warpSpill(lane, buf, n, out);
   if (pass) buf[n + (uint32_t)__popc(mask & laneMaskLt())] = make_uint2(j, k);
   n += (uint32_t)__popc(mask);
 }
@@ -103,9 +148,7 @@ __device__ __forceinline__ int windowOwner(uint32_t excl, uint32_t item) {
 // round however uneven the windows are.
 __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int lane, int warpBase,
                                                 const float4 *__restrict__ posf, float cutF, uint2 *sCandW,
-                                                uint32_t &nBuf, uint2 *__restrict__ cand,
-                                                unsigned long long *__restrict__ candCount,
-                                                unsigned long long candCap) {
+                                                uint32_t &nBuf, const CandSink &out) {
   const uint32_t cnt = hi - lo;
   uint32_t incl = cnt;
 #pragma unroll
@@ -121,7 +164,7 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
     const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
     const uint32_t jj = (uint32_t)(warpBase + owner), k = oLo + (item - oEx);
     const bool pass = item < total && prefilterPass(__ldg(&posf[jj]), __ldg(&posf[k]), cutF);
-    warpAppend(pass, jj, k, lane, sCandW, nBuf, cand, candCount, candCap);
+    warpAppend(pass, jj, k, lane, sCandW, nBuf, out);
   }
 }
 
@@ -133,12 +176,9 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
                                                               const uint32_t *__restrict__ skeys,
                                                               const uint32_t *__restrict__ rowStart,
                                                               const uint16_t *__restrict__ cellOff, GridDesc g,
-                                                              double cutoffSq, double nearRel, float cutF,
-                                                              uint32_t denseMin,
+                                                              float cutF, uint32_t denseMin,
                                                               const uint32_t *__restrict__ denseCount,
-                                                              uint2 *__restrict__ cand,
-                                                              unsigned long long *__restrict__ candCount,
-                                                              unsigned long long candCap) {
+                                                              const CandSink out) {
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
@@ -180,10 +220,10 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
           rowWindow(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo, hi);
         }
       }
-      warpWindowPairs(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, cand, candCount, candCap);
+      warpWindowPairs(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
     }
   }
-  warpFlush(lane, sCand[warp], nBuf, cand, candCount, candCap);
+  warpFlush(lane, sCand[warp], nBuf, out);
 }
 
 // Dense bin of the pair scan (cells with >= kDenseCell objects, listed by the
@@ -217,10 +257,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
                                                          const uint32_t *__restrict__ skeys,
                                                          const uint32_t *__restrict__ rowStart,
                                                          const uint16_t *__restrict__ cellOff, GridDesc g,
-                                                         double cutoffSq, double nearRel, float cutF,
-                                                         uint2 *__restrict__ cand,
-                                                         unsigned long long *__restrict__ candCount,
-                                                         unsigned long long candCap) {
+                                                         float cutF, const CandSink out) {
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
   __shared__ float4 sNb[kScanCta / 32][kTileStage];
   __shared__ uint32_t sK[kScanCta / 32][kTileStage];
@@ -289,33 +326,34 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
           const uint32_t k = sK[warp][u];
           const bool pass = src && prefilterPass(mf, qq, cutF) &&
                             !(stBase + u < ownEnd && k <= si);  // own row: later objects only
-          warpAppend(pass, si, k, lane, sCand[warp], nBuf, cand, candCount, candCap);
+          warpAppend(pass, si, k, lane, sCand[warp], nBuf, out);
         }
       }
       __syncwarp();
     }
   }
-  warpFlush(lane, sCand[warp], nBuf, cand, candCount, candCap);
+  warpFlush(lane, sCand[warp], nBuf, out);
 }
 
 
-// grid-stride over the candidates (count read on the device)
+// grid-stride over both candidate lists (lengths read on the device; see CandSink)
 __global__ void __launch_bounds__(256) k_pair_eval(ScanPack pk, const uint2 *__restrict__ cand,
                                                    const unsigned long long *__restrict__ candCount,
-                                                   unsigned long long candCap,
+                                                   unsigned long long half,
                                                    unsigned long long *__restrict__ candNeed, ScanConsts c,
                                                    const int64_t *__restrict__ iterPtr, int64_t iterOffset,
                                                    ladds_pair *__restrict__ out,
                                                    unsigned long long *__restrict__ count, unsigned long long cap) {
-  const unsigned long long total = *candCount;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(candNeed, total);
-  const unsigned long long m = total < candCap ? total : candCap;
+  const unsigned long long t0 = candCount[0], t1 = candCount[1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(candNeed, t0 > t1 ? t0 : t1);
+  const unsigned long long m0 = t0 < half ? t0 : half, m1 = t1 < half ? t1 : half;
   const int64_t it = *iterPtr + iterOffset;  // iteration index stored in the records
   const uint32_t step = it < 0 ? 0u : (uint32_t)it;
-  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < m;
+  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < m0 + m1;
        q += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint2 p = cand[q];
-    if (!mayRecord(c, pk.posf[p.x], pk.velf[p.x], pk.posf[p.y], pk.velf[p.y])) continue;
+    const bool screened = q < m0;
+    const uint2 p = cand[screened ? q : half + (q - m0)];
+    if (!screened && !mayRecord(c, pk.posf[p.x], pk.velf[p.x], pk.posf[p.y], pk.velf[p.y])) continue;
     Obj a, b;
     loadObjPacked(pk, p.x, a);
     loadObjPacked(pk, p.y, b);
