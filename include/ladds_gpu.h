@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define LADDS_GPU_ABI_VERSION 1
+#define LADDS_GPU_ABI_VERSION 2
 
 /* ---- status codes ---- */
 #define LADDS_OK 0
@@ -111,7 +111,19 @@ typedef struct {
   int32_t scanBlock;              /* threads per block of the candidate evaluation (0: 256) */
   int32_t useGraphs;              /* capture multi-iteration calls in CUDA graphs      */
   uint64_t pairCapacity;          /* initial device pair-buffer capacity (0: auto)     */
+  int32_t scanScreen;             /* LADDS_SCREEN_*: how the pair scan screens full
+                                     candidate buffers (results do not depend on it)   */
 } ladds_gpu_config;
+
+/* The binary32 closest-approach screen of the pre-filtered pairs (a superset
+ * test: it drops only pairs that provably yield no record) runs on each warp's
+ * buffer of pre-filtered pairs at the end of the candidate walk, and a buffer
+ * that fills up during the walk is either listed unscreened for the evaluation
+ * kernel (LISTS: sparse populations, about one pre-filtered pair per object)
+ * or screened where it is (BUFFER: dense populations, tens of pre-filtered
+ * pairs per object). */
+#define LADDS_SCREEN_LISTS 0
+#define LADDS_SCREEN_BUFFER 1
 
 typedef struct ladds_gpu_ctx ladds_gpu_ctx;
 
@@ -380,6 +392,7 @@ typedef struct {
   double cellSize;          /* cell edge used [km] */
   int32_t reach;            /* neighbour reach in cells */
   int32_t propagateBlock, scanBlock, chunkSteps;
+  int32_t scanScreen;       /* LADDS_SCREEN_* */
   double msPerStep;         /* device time per iteration of the trial */
 } ladds_tune_trial;
 int ladds_gpu_autotune(ladds_gpu_ctx *ctx, int stepsPerTrial, ladds_tune_trial *trials, size_t cap, size_t *nTrials,

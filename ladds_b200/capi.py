@@ -23,6 +23,7 @@ KEP, J2, C22, S22, SOL, LUN, SRP, DRAG, J3 = (1 << k for k in range(9))
 PROP_ALL = 0x1FF
 PASSIVE, EVASIVE, EVASIVE_PRESERVING = 0, 1, 2
 PRECISION_FP64, PRECISION_SPLIT = 0, 1
+SCREEN_LISTS, SCREEN_BUFFER = 0, 1
 PAIR_COLLISION, PAIR_EVASION, PAIR_CONJUNCTION = 1, 2, 4
 PAIR_NEAR_COLLISION, PAIR_NEAR_EVASION, PAIR_NEAR_CONJUNCTION, PAIR_NEAR_GATE = 8, 16, 32, 64
 SIZE_MAX = np.uint64(0xFFFFFFFFFFFFFFFF)
@@ -60,6 +61,7 @@ class GpuConfig(C.Structure):
         ("scanBlock", C.c_int32),
         ("useGraphs", C.c_int32),
         ("pairCapacity", C.c_uint64),
+        ("scanScreen", C.c_int32),
     ]
 
 
@@ -111,7 +113,8 @@ assert OBJECT_DTYPE.itemsize == 80
 
 class TuneTrial(C.Structure):
     _fields_ = [("cellSize", C.c_double), ("reach", C.c_int32), ("propagateBlock", C.c_int32),
-                ("scanBlock", C.c_int32), ("chunkSteps", C.c_int32), ("msPerStep", C.c_double)]
+                ("scanBlock", C.c_int32), ("chunkSteps", C.c_int32), ("scanScreen", C.c_int32),
+                ("msPerStep", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -541,18 +541,21 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
     cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
     const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap};
-    k_pair_candidates<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
+    const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
+    (buffer ? k_pair_candidates<LADDS_SCREEN_BUFFER>
+            : k_pair_candidates<LADDS_SCREEN_LISTS>)<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
         c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF,
         dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, out);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
-      k_pair_tiles<<<4 * c->evalBlocks, kScanCta, 0, s>>>(dense.cells, dense.count, dense.cap, c->cur.tag,
-                                                      c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
-                                                      cutF, out);
+      (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
+              : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(
+          dense.cells, dense.count, dense.cap, c->cur.tag, c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
+          cutF, out);
   }
   PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
-  // grid-stride over the screened candidates (their count is only known on the device; few per step)
-  const int evalGrid = std::max(1, std::min(blocksFor(c->candCap, b), c->evalBlocks / 2));
+  // grid-stride over both candidate lists (their lengths are only known on the device): one resident wave
+  const int evalGrid = std::max(1, std::min(blocksFor(2 * c->candCap, b), c->evalBlocks * 256 / b));
   k_pair_eval<<<evalGrid, b, 0, s>>>(scanPack(c), c->dCand, c->dCandCount, (unsigned long long)c->candCap,
                                      c->dCandNeed, sc, iterPtr, iterOffset, c->dPairs, c->dCount,
                                      (unsigned long long)c->pairCap);
@@ -763,6 +766,7 @@ void ladds_gpu_config_default(ladds_gpu_config *f) {
   f->scanBlock = 256;
   f->useGraphs = 1;
   f->pairCapacity = 0;
+  f->scanScreen = LADDS_SCREEN_LISTS;
 }
 
 const char *ladds_gpu_last_error(const ladds_gpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
@@ -775,7 +779,8 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       (f->componentMask & ~LADDS_PROP_ALL) || !(f->nearThresholdRel >= 0))
     return LADDS_ERR_INVALID_ARG;
   if (f->propagateBlock < 0 || f->propagateBlock > 256 || (f->propagateBlock % 32) || f->scanBlock < 0 ||
-      f->scanBlock > 256 || (f->scanBlock % 32))
+      f->scanBlock > 256 || (f->scanBlock % 32) ||
+      (f->scanScreen != LADDS_SCREEN_LISTS && f->scanScreen != LADDS_SCREEN_BUFFER))
     return LADDS_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -1578,6 +1583,7 @@ int tuneTrial(ladds_gpu_ctx *c, const ladds_gpu_config &cfg, int chunk, int step
     t.propagateBlock = cfg.propagateBlock;
     t.scanBlock = cfg.scanBlock;
     t.chunkSteps = chunk;
+    t.scanScreen = cfg.scanScreen;
     t.msPerStep = st.deviceMs / std::max(steps, 1);
   }
   ladds_gpu_destroy(tc);
@@ -1610,17 +1616,29 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
     }
     return LADDS_OK;
   };
+  // 0. where full candidate buffers are screened (the population's density
+  //    decides), at the current cell edge
+  {
+    const ladds_gpu_config base = cfg;
+    for (int screen : {LADDS_SCREEN_LISTS, LADDS_SCREEN_BUFFER}) {
+      ladds_gpu_config k = base;
+      k.scanScreen = screen;
+      const int rc = run(k, bestChunk);
+      if (rc) return rc;
+    }
+  }
   // 1. cell edge in [20, 160] km: cutoff / R (neighbour reach R = 1..4) and
-  //    coarser cells 1.5 and 2 cutoffs wide (reach 1); the current edge as well
+  //    coarser cells 1.5 and 2 cutoffs wide (reach 1); the current edge is
+  //    measured already
   {
     const ladds_gpu_config base = cfg;
     std::vector<double> cells = {base.cellSize};
     for (int R = 1; R <= 4; ++R) cells.push_back(base.cutoff * (1.0 + 1e-6) / R);
     cells.push_back(1.5 * base.cutoff);
     cells.push_back(2.0 * base.cutoff);
-    for (size_t i = 0; i < cells.size(); ++i) {
+    for (size_t i = 1; i < cells.size(); ++i) {
       const double cs = cells[i];
-      if (i > 0 && (cs < 20.0 || cs > 160.0)) continue;
+      if (cs < 20.0 || cs > 160.0) continue;
       if (i == 1 && base.cellSize <= 0) continue;  // the default edge: measured as the current one
       if (i > 1 && cs == base.cellSize) continue;
       ladds_gpu_config k = base;
@@ -1661,6 +1679,7 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
   c->cfg.cellSize = cfg.cellSize;
   c->cfg.propagateBlock = cfg.propagateBlock;
   c->cfg.scanBlock = cfg.scanBlock;
+  c->cfg.scanScreen = cfg.scanScreen;
   c->chunkSteps = bestChunk;
   dropGraphs(c);
   if (regrid) {

@@ -13,9 +13,13 @@
 // buffer 32 pairs at a time with the binary32 closest-approach test mayRecord
 // and appends the few pairs that can yield a record to the screened list; a
 // buffer that fills up during the walk is appended unscreened to the second
-// list (keeping the screen out of the walk's registers).  Objects of cells with
-// >= kDenseCell objects are sources of k_pair_tiles instead (the occupancy bin
-// of crowded cells).
+// list (keeping the screen out of the walk's registers).  Dense populations
+// (tens of pre-filtered pairs per object) take the LADDS_SCREEN_BUFFER form
+// instead: a full buffer is screened where it is, so that no unscreened pair
+// goes through global memory, at the price of the screen's registers in the
+// walk (the autotuner picks the form).  Objects of cells with >= kDenseCell
+// objects are sources of k_pair_tiles instead (the occupancy bin of crowded
+// cells).
 //
 // Phase 2, k_pair_eval: one thread per listed candidate (unscreened ones are
 // screened first) applies the exact binary64 cutoff gate d^2 <= cutoff^2
@@ -78,7 +82,8 @@ struct CandSink {
 // register (warp-uniform): appends are ballots, no atomics.  Every lane of the
 // warp calls these.
 //
-// A full buffer during the walk: appended unscreened with one global atomic.
+// A full buffer during the walk (LADDS_SCREEN_LISTS): appended unscreened to
+// the second list with one global atomic.
 __device__ __forceinline__ void warpSpill(int lane, uint2 *buf, uint32_t &n, const CandSink &out) {
   __syncwarp();
   if (n) {
@@ -94,9 +99,10 @@ __device__ __forceinline__ void warpSpill(int lane, uint2 *buf, uint32_t &n, con
   n = 0;
 }
 
-// The buffer at the end of the walk: screened 32 pairs at a time (all four
-// loads of a lane in flight together); the survivors are appended with one
-// global atomic per round that has any.
+// The buffer at the end of the walk (and, LADDS_SCREEN_BUFFER, whenever it is
+// full): screened 32 pairs at a time (all four loads of a lane in flight
+// together); the survivors are appended to the screened list with one global
+// atomic per round that has any.
 __device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, const CandSink &out) {
   __syncwarp();
   for (uint32_t b = 0; b < n; b += 32u) {
@@ -121,11 +127,17 @@ __device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, con
   n = 0;
 }
 
+template <int SCREEN>
 __device__ __forceinline__ void warpAppend(bool pass, uint32_t j, uint32_t k, int lane, uint2 *buf, uint32_t &n,
                                            const CandSink &out) {
   const uint32_t mask = __ballot_sync(0xffffffffu, pass);
   if (!mask) return;
-  if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) warpSpill(lane, buf, n, out);
+  if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) {
+    if (SCREEN == LADDS_SCREEN_BUFFER)
+      warpFlush(lane, buf, n, out);
+    else
+      warpSpill(lane, buf, n, out);
+  }
   if (pass) buf[n + (uint32_t)__popc(mask & laneMaskLt())] = make_uint2(j, k);
   n += (uint32_t)__popc(mask);
 }
@@ -146,6 +158,7 @@ __device__ __forceinline__ int windowOwner(uint32_t excl, uint32_t item) {
 // its object; the windows of the warp are concatenated (exclusive prefix
 // `excl`) and dealt out 32 items per round, so every lane tests one pair per
 // round however uneven the windows are.
+template <int SCREEN>
 __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int lane, int warpBase,
                                                 const float4 *__restrict__ posf, float cutF, uint2 *sCandW,
                                                 uint32_t &nBuf, const CandSink &out) {
@@ -164,13 +177,14 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
     const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
     const uint32_t jj = (uint32_t)(warpBase + owner), k = oLo + (item - oEx);
     const bool pass = item < total && prefilterPass(__ldg(&posf[jj]), __ldg(&posf[k]), cutF);
-    warpAppend(pass, jj, k, lane, sCandW, nBuf, out);
+    warpAppend<SCREEN>(pass, jj, k, lane, sCandW, nBuf, out);
   }
 }
 
 // cutF: cutoff * (1 + nearRel) rounded up, so that every pair the exact gate or
 // its near band accepts passes the binary32 test.  The loops over the
 // neighbour rows are warp-uniform; inactive lanes contribute empty windows.
+template <int SCREEN>
 __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__restrict__ tags,
                                                               const float4 *__restrict__ posf, int n,
                                                               const uint32_t *__restrict__ skeys,
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
           rowWindow(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo, hi);
         }
       }
-      warpWindowPairs(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
+      warpWindowPairs<SCREEN>(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
     }
   }
   warpFlush(lane, sCand[warp], nBuf, out);
@@ -250,6 +264,7 @@ __device__ __forceinline__ int halfShellRowOf(int q, int R, int &dz, int &dy) {
   return q;
 }
 
+template <int SCREEN>
 __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restrict__ denseCells,
                                                          const uint32_t *__restrict__ denseCount, uint32_t denseCap,
                                                          const uint32_t *__restrict__ tags,
@@ -326,7 +341,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
           const uint32_t k = sK[warp][u];
           const bool pass = src && prefilterPass(mf, qq, cutF) &&
                             !(stBase + u < ownEnd && k <= si);  // own row: later objects only
-          warpAppend(pass, si, k, lane, sCand[warp], nBuf, out);
+          warpAppend<SCREEN>(pass, si, k, lane, sCand[warp], nBuf, out);
         }
       }
       __syncwarp();

@@ -117,11 +117,12 @@ DENSE_KW = dict(cutoff=20.0, collisionDistanceFactor=2000.0, minDetectionRadius=
                 conjunctionThreshold=2.0, boxMin=DENSE_BOX[0], boxMax=DENSE_BOX[1])
 
 
+@pytest.mark.parametrize("screen", [0, 1])
 @pytest.mark.parametrize("cell", [0.0, 7.0, 10.0, 33.0, 60.0])
-def test_scan_bitexact_vs_oracle(capi, oracle, cell):
+def test_scan_bitexact_vs_oracle(capi, oracle, cell, screen):
     pop = dense_population(11)
     dt = 10.0
-    with ctx_for(capi, cellSize=cell, **DENSE_KW) as ctx:
+    with ctx_for(capi, cellSize=cell, scanScreen=screen, **DENSE_KW) as ctx:
         ctx.upload(pop)
         recs = ctx.conjunctions(dt)
         keys, slots = ctx.cell_order()
@@ -144,8 +145,9 @@ def test_scan_bitexact_vs_oracle(capi, oracle, cell):
     assert np.array_equal(keys, okeys[operm])
 
 
+@pytest.mark.parametrize("screen", [0, 1])
 @pytest.mark.parametrize("cell", [0.0, 10.0])
-def test_scan_dense_cells_bitexact(capi, oracle, cell):
+def test_scan_dense_cells_bitexact(capi, oracle, cell, screen):
     """Cells of hundreds of objects (the dense bin, scanned by cell tiles) next
     to sparse cells (the per-object walk): records bit-exact vs the oracle."""
     rng = np.random.default_rng(5)
@@ -158,7 +160,7 @@ def test_scan_dense_cells_bitexact(capi, oracle, cell):
         parts.append(c)
     pop = {k: np.concatenate([p_[k] for p_ in parts]) for k in parts[0]}
     pop["id"] = np.arange(len(pop["x"]), dtype=np.uint64)
-    with ctx_for(capi, cellSize=cell, **DENSE_KW) as ctx:
+    with ctx_for(capi, cellSize=cell, scanScreen=screen, **DENSE_KW) as ctx:
         ctx.upload(pop)
         recs = ctx.conjunctions(10.0)
     p = oracle.scan_params(cutoff=20.0, dt=10.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
@@ -311,11 +313,13 @@ def test_propagation_vs_oracle_100_steps(capi, oracle, mask_name, precision):
     assert np.array_equal(got["id"], pop["id"])
 
 
-def test_graph_replay_equals_eager(capi):
+@pytest.mark.parametrize("screen", [0, 1])
+def test_graph_replay_equals_eager(capi, screen):
     pop = dense_population(14, n=5000)
     outs = []
     for graphs in (0, 1):
-        with ctx_for(capi, useGraphs=graphs, deltaT=1.0, componentMask=capi.KEP | capi.J2, **DENSE_KW) as ctx:
+        with ctx_for(capi, useGraphs=graphs, deltaT=1.0, componentMask=capi.KEP | capi.J2, scanScreen=screen,
+                     **DENSE_KW) as ctx:
             ctx.upload(pop)
             r1 = ctx.step(7)
             r2 = ctx.step(7)  # second call replays the cached graph
