@@ -542,15 +542,17 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
     const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap};
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
+    // the largest separation a record or a near-band flag can have, with room for rounding
+    const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
     (buffer ? k_pair_candidates<LADDS_SCREEN_BUFFER>
             : k_pair_candidates<LADDS_SCREEN_LISTS>)<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
-        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF,
+        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF, reach * reach,
         dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, out);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
               : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(
           dense.cells, dense.count, dense.cap, c->cur.tag, c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
-          cutF, out);
+          cutF, reach * reach, out);
   }
   PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;

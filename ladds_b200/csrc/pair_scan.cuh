@@ -34,25 +34,79 @@ namespace ladds {
 constexpr int kScanCta = 128;
 constexpr int kWarpCand = 128;  // candidates buffered per warp before a global append
 
+// The four reads that locate the cells xlo..xhi of row r2 in the sorted
+// arrays (row start and end, offsets of the two cells inside the row), issued
+// together: none waits for another.  Offsets of a row that the table does not
+// cover are read but not used.
+struct RowLookup {
+  uint32_t rs0, rs1, o0, o1;
+};
+__device__ __forceinline__ RowLookup rowLoads(uint32_t r2, uint32_t xlo, uint32_t xhi, uint32_t nx,
+                                              const uint32_t *__restrict__ rowStart,
+                                              const uint16_t *__restrict__ cellOff) {
+  RowLookup L;
+  L.rs0 = __ldg(&rowStart[r2]);
+  L.rs1 = __ldg(&rowStart[r2 + 1]);
+  L.o0 = L.o1 = 0u;
+  if (cellOff) {
+    const uint16_t *t = cellOff + (size_t)r2 * cellOffPitch(nx);
+    L.o0 = __ldg(&t[xlo]);
+    L.o1 = __ldg(&t[xhi + 1]);
+  }
+  return L;
+}
+
+// [lo, hi) of the cells xlo..xhi of row r2 from its lookups; rows whose
+// offsets do not fit 16 bits (or no table) search the sorted keys
+__device__ __forceinline__ void rowFinish(const RowLookup &L, uint32_t r2, uint32_t xlo, uint32_t xhi, uint32_t nx,
+                                          const uint16_t *__restrict__ cellOff, const uint32_t *__restrict__ skeys,
+                                          uint32_t &lo, uint32_t &hi) {
+  if (L.rs1 == L.rs0) {
+    lo = hi = L.rs0;
+  } else if (cellOff && L.rs1 - L.rs0 <= 65535u) {
+    lo = L.rs0 + L.o0;
+    hi = L.rs0 + L.o1;
+  } else {
+    const uint32_t rowBase = r2 * nx;
+    lo = lowerBound(skeys, L.rs0, L.rs1, rowBase + xlo);
+    hi = lowerBound(skeys, lo, L.rs1, rowBase + xhi + 1);
+  }
+}
+
 // [lo, hi) of the cells xlo..xhi of row r2 in the sorted arrays
 __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xhi, uint32_t nx,
                                           const uint32_t *__restrict__ rowStart,
                                           const uint16_t *__restrict__ cellOff,
                                           const uint32_t *__restrict__ skeys, uint32_t &lo, uint32_t &hi) {
-  const uint32_t rs0 = __ldg(&rowStart[r2]), rs1 = __ldg(&rowStart[r2 + 1]);
-  if (rs1 == rs0) {
-    lo = hi = rs0;
-    return;
-  }
-  if (cellOff && rs1 - rs0 <= 65535u) {
-    const uint16_t *t = cellOff + (size_t)r2 * cellOffPitch(nx);
-    lo = rs0 + __ldg(&t[xlo]);
-    hi = rs0 + __ldg(&t[xhi + 1]);
+  rowFinish(rowLoads(r2, xlo, xhi, nx, rowStart, cellOff), r2, xlo, xhi, nx, cellOff, skeys, lo, hi);
+}
+
+// half-shell row q of a reach-R walk: the own row (dz, dy) = (0, 0), the rows
+// (0, 1..R), then (dz, -R..R) for dz = 1..R
+__device__ __forceinline__ void halfShellRowOf(int q, int R, int &dz, int &dy) {
+  if (q <= R) {
+    dz = 0;
+    dy = q;
   } else {
-    const uint32_t rowBase = r2 * nx;
-    lo = lowerBound(skeys, rs0, rs1, rowBase + xlo);
-    hi = lowerBound(skeys, lo, rs1, rowBase + xhi + 1);
+    const int t = q - (R + 1);
+    dz = 1 + t / (2 * R + 1);
+    dy = t % (2 * R + 1) - R;
   }
+}
+
+// Cells (dx, dy, dz) apart hold points at least c sqrt(a^2 + b^2 + e^2) apart,
+// a = max(|dx| - 1, 0), b and e likewise (an object clamped into a boundary
+// cell of the grid lies outside it, farther away still): the x half-width of
+// the neighbour row (dy, dz) that can hold partners within sqrt(reachR2), -1
+// if none.  The corner rows and columns of the (2R+1)^3 block drop out for
+// R >= 3.
+__device__ __forceinline__ int rowHalfWidth(int dy, int dz, int R, double c2, double reachR2) {
+  const int b = max(abs(dy) - 1, 0), e = max(abs(dz) - 1, 0);
+  const double m = (double)(b * b + e * e) * c2;
+  if (m > reachR2) return -1;
+  int w = R;
+  while (w > 1 && m + (double)((w - 1) * (w - 1)) * c2 > reachR2) --w;
+  return w;
 }
 
 // Binary32 pre-filter of one candidate pair with its positions loaded.  The
@@ -190,7 +244,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
                                                               const uint32_t *__restrict__ skeys,
                                                               const uint32_t *__restrict__ rowStart,
                                                               const uint16_t *__restrict__ cellOff, GridDesc g,
-                                                              float cutF, uint32_t denseMin,
+                                                              float cutF, double reachR2, uint32_t denseMin,
                                                               const uint32_t *__restrict__ denseCount,
                                                               const CandSink out) {
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
@@ -218,20 +272,23 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
       }
     }
   }
-  const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
+  const double c2 = g.cellSize * g.cellSize;
   for (int dz = 0; dz <= R; ++dz) {
     for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
+      const int w = rowHalfWidth(dy, dz, R, c2, reachR2);  // warp-uniform
+      if (w < 0) continue;
       const int32_t jz = iz + dz, jy = iy + dy;
+      const bool ok = active && jz < nz && jy >= 0 && jy < ny;
+      const uint32_t r2 = ok ? (uint32_t)jz * (uint32_t)ny + (uint32_t)jy : 0u;
+      const uint32_t xlo = ok ? (dz == 0 && dy == 0 ? (uint32_t)ix : (uint32_t)max(ix - w, 0)) : 0u;
+      const uint32_t xhi = ok ? (uint32_t)min(ix + w, nx - 1) : 0u;
+      const RowLookup L = rowLoads(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff);  // four reads in flight
       uint32_t lo = 0, hi = 0;
-      if (active && jz < nz && jy >= 0 && jy < ny) {
-        const uint32_t r2 = (uint32_t)jz * (uint32_t)ny + (uint32_t)jy;
-        if (dz == 0 && dy == 0) {
-          uint32_t l0;
-          rowWindow(r2, (uint32_t)ix, xhi, (uint32_t)nx, rowStart, cellOff, skeys, l0, hi);
-          lo = (uint32_t)j + 1u;  // own cell: later objects only
+      if (ok) {
+        rowFinish(L, r2, xlo, xhi, (uint32_t)nx, cellOff, skeys, lo, hi);
+        if (dz == 0 && dy == 0) {  // own cell: later objects only
+          lo = (uint32_t)j + 1u;
           if (hi < lo) hi = lo;
-        } else {
-          rowWindow(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo, hi);
         }
       }
       warpWindowPairs<SCREEN>(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
@@ -252,18 +309,6 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
 // candidate output as k_pair_candidates, which skips these objects as sources.
 constexpr uint32_t kTileStage = 256;  // staged neighbour objects per warp and pass
 
-__device__ __forceinline__ int halfShellRowOf(int q, int R, int &dz, int &dy) {
-  if (q <= R) {
-    dz = 0;
-    dy = q;
-  } else {
-    const int t = q - (R + 1);
-    dz = 1 + t / (2 * R + 1);
-    dy = t % (2 * R + 1) - R;
-  }
-  return q;
-}
-
 template <int SCREEN>
 __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restrict__ denseCells,
                                                          const uint32_t *__restrict__ denseCount, uint32_t denseCap,
@@ -272,7 +317,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
                                                          const uint32_t *__restrict__ skeys,
                                                          const uint32_t *__restrict__ rowStart,
                                                          const uint16_t *__restrict__ cellOff, GridDesc g,
-                                                         float cutF, const CandSink out) {
+                                                         float cutF, double reachR2, const CandSink out) {
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
   __shared__ float4 sNb[kScanCta / 32][kTileStage];
   __shared__ uint32_t sK[kScanCta / 32][kTileStage];
@@ -288,7 +333,6 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
     const uint32_t r = key / (uint32_t)nx;
     const int32_t ix = (int32_t)(key - r * (uint32_t)nx), iy = (int32_t)(r % (uint32_t)ny),
                   iz = (int32_t)(r / (uint32_t)ny);
-    const uint32_t xlo = (uint32_t)max(ix - R, 0), xhi = (uint32_t)min(ix + R, nx - 1);
     const uint32_t rs = __ldg(&rowStart[r]);
     const uint16_t *t = cellOff + (size_t)r * pitch;
     const uint32_t c0 = rs + __ldg(&t[ix]), c1 = rs + __ldg(&t[ix + 1]);
@@ -298,7 +342,9 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
       int dz, dy;
       halfShellRowOf(lane, R, dz, dy);
       const int32_t jz = iz + dz, jy = iy + dy;
-      if (jz < nz && jy >= 0 && jy < ny) {
+      const int w = rowHalfWidth(dy, dz, R, g.cellSize * g.cellSize, reachR2);
+      const uint32_t xlo = (uint32_t)max(ix - w, 0), xhi = (uint32_t)min(ix + w, nx - 1);
+      if (w >= 0 && jz < nz && jy >= 0 && jy < ny) {
         if (lane == 0) {
           lo = c0;
           hi = rs + __ldg(&t[xhi + 1]);
