@@ -227,6 +227,30 @@ int ladds_gpu_mark_deleted(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t n);
 /* Sets every parentId to SIZE_MAX (Simulation.cpp:470-473). */
 int ladds_gpu_clear_parents(ladds_gpu_ctx *ctx);
 
+/* ---- slab decomposition over ranks (driver: ladds_b200/slabs.py) ----
+ * Replaces the domain decomposition of LADDS' MPI mode
+ * (distributedMemParallelization/AltitudeBasedDecomposition.cpp:131-179,
+ * RegularGridDecomposition.cpp) and the migrant checks of
+ * ParticleMigrationHandler.cpp:11-56 (called at Simulation.cpp:313-376) for a
+ * cell grid: rank r owns the objects of the cell layers [z_r, z_{r+1}) (layer
+ * iz = the z index of the cell key) and scans them together with a halo, the
+ * next rank's lowest `reach` layers, so that the ranks' record sets are the
+ * single-context set exactly.
+ *
+ * Slots (ascending) of the live objects whose cell layer lies in [izLo, izHi);
+ * *n = their count (LADDS_ERR_CAPACITY if it exceeds cap). */
+int ladds_gpu_select_layers(ladds_gpu_ctx *ctx, int32_t izLo, int32_t izHi, uint32_t *slots, size_t cap, size_t *n);
+/* Live objects per cell layer; counts has nLayers >= dims[2] entries. */
+int ladds_gpu_layer_histogram(ladds_gpu_ctx *ctx, uint64_t *counts, size_t nLayers);
+/* Removes the objects with the given slots (emigrants, a scanned halo); the
+ * others keep their relative slot order and are renumbered 0..n'-1. */
+int ladds_gpu_remove_slots(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t m);
+/* Objects with slot >= haloStart are halo: targets of the pair scan, never
+ * its sources, so that halo-halo pairs are not scanned.  Halo objects must lie
+ * in higher cell layers than every other object (the layers above a slab):
+ * the half-shell walk finds a pair from its lower object.  SIZE_MAX: no halo. */
+int ladds_gpu_set_halo(ladds_gpu_ctx *ctx, size_t haloStart);
+
 /* ---- explicit pair lists (the AoSFunctor call shape) ---- */
 /* One object of a pair evaluation (80 bytes). */
 typedef struct {

@@ -87,7 +87,8 @@ EXPORTED = [
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
     "ladds_records_write_csv", "ladds_gpu_checked_insert", "ladds_gpu_get_objects", "ladds_breakup_collision",
-    "ladds_gpu_breakup",
+    "ladds_gpu_breakup", "ladds_gpu_select_layers", "ladds_gpu_layer_histogram", "ladds_gpu_remove_slots",
+    "ladds_gpu_set_halo",
 ]
 
 STATE_RECORD_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("aom", "<f8"),
@@ -178,6 +179,10 @@ def lib():
     L.ladds_records_pack.argtypes = [vp, sz, C.c_uint32, vp, sz, C.POINTER(sz)]
     L.ladds_records_write_csv.argtypes = [C.c_char_p, i, vp, sz, C.c_uint32]
     L.ladds_gpu_autotune.argtypes = [vp, i, C.POINTER(TuneTrial), sz, C.POINTER(sz), C.POINTER(TuneTrial)]
+    L.ladds_gpu_select_layers.argtypes = [vp, C.c_int32, C.c_int32, vp, sz, C.POINTER(sz)]
+    L.ladds_gpu_layer_histogram.argtypes = [vp, vp, sz]
+    L.ladds_gpu_remove_slots.argtypes = [vp, vp, sz]
+    L.ladds_gpu_set_halo.argtypes = [vp, sz]
     L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
     return L
@@ -391,6 +396,29 @@ class Context:
 
     def clear_parents(self):
         self._check(self._L.ladds_gpu_clear_parents(self._h))
+
+    # ---- slab decomposition primitives (ladds_b200.slabs)
+    def select_layers(self, iz_lo: int, iz_hi: int) -> np.ndarray:
+        """Slots (ascending) of the live objects in the cell layers [iz_lo, iz_hi)."""
+        cap = max(self.size(), 1)
+        out = np.zeros(cap, dtype=np.uint32)
+        n = C.c_size_t()
+        self._check(self._L.ladds_gpu_select_layers(self._h, iz_lo, iz_hi, _p(out), cap, C.byref(n)))
+        return out[: n.value].copy()
+
+    def layer_histogram(self) -> np.ndarray:
+        nz = self.grid()[0][2]
+        out = np.zeros(nz, dtype=np.uint64)
+        self._check(self._L.ladds_gpu_layer_histogram(self._h, _p(out), nz))
+        return out
+
+    def remove_slots(self, slots):
+        slots = np.ascontiguousarray(slots, dtype=np.uint32)
+        self._check(self._L.ladds_gpu_remove_slots(self._h, _p(slots), len(slots)))
+
+    def set_halo(self, halo_start: int | None):
+        """Objects with slot >= halo_start are pair-scan targets only (None: no halo)."""
+        self._check(self._L.ladds_gpu_set_halo(self._h, (1 << 64) - 1 if halo_start is None else halo_start))
 
     def scan(self, params: ScanParams, cap: int = 4096):
         """Conjunction scan of the current state with explicit functor scalars."""

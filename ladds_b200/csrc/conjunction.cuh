@@ -280,6 +280,18 @@ __global__ void k_burnup_flags(const double *__restrict__ x, const double *__res
   if (tagSlot(tag[j]) < (uint32_t)n) aliveBySlot[tagSlot(tag[j])] = k;
 }
 
+// keep[j] = 0 for the objects whose slot is marked (slotMark[slot] = 1);
+// aliveBySlot mirrors it in slot order.
+__global__ void k_slot_mark_flags(const uint32_t *__restrict__ tag, int n, const uint8_t *__restrict__ slotMark,
+                                  uint32_t *__restrict__ keep, uint32_t *__restrict__ aliveBySlot) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t s = tagSlot(tag[j]);
+  const uint32_t k = (s < (uint32_t)n && slotMark[s]) ? 0u : 1u;
+  keep[j] = k;
+  if (s < (uint32_t)n) aliveBySlot[s] = k;
+}
+
 // compaction: dst[pos[j]] = src[j] for kept j; slots renumbered via newSlot
 __global__ void k_compact(DevState src, DevState dst, const uint32_t *__restrict__ keep,
                           const uint32_t *__restrict__ pos, const uint32_t *__restrict__ newSlot, int n) {

@@ -113,6 +113,7 @@ struct ladds_gpu_ctx {
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
   int chunkSteps = kMaxEphSteps;  // iterations per ephemeris chunk / captured graph (autotuned)
   uint32_t *denseCells = nullptr, *denseCount = nullptr;  // dense bin of the pair scan (cells >= kDenseCell)
+  uint32_t haloStart = 0xffffffffu;  // objects with slot >= haloStart: pair-scan targets only
   uint32_t denseCap = 0;
   // second set of the sort results: the sort of a step writes one set while the
   // pair scan of the previous step still reads the other
@@ -540,7 +541,7 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
   {
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
     cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
-    const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap};
+    const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap, c->haloStart};
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
     // the largest separation a record or a near-band flag can have, with room for rounding
     const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
@@ -1177,6 +1178,34 @@ int ladds_gpu_integrate(ladds_gpu_ctx *c, int steps) {
 }  // extern "C"
 
 namespace {
+// Compaction of the objects flagged keep[j] = 1 in scratchA (current order;
+// scratchC holds the same flags in slot order): survivors keep their
+// relative slot order and are renumbered 0..n'-1; the pre-compaction state
+// is left in c->alt.  hKeep (may be NULL) receives the flags.
+int compactKept(ladds_gpu_ctx *c, std::vector<uint32_t> *hKeep) {
+  const int n = (int)c->n;
+  uint32_t *keep = c->scratchA, *pos = c->scratchB, *aliveBySlot = c->scratchC, *newSlot = c->keys1;
+  // exclusive scans: positions in the current order, new slot numbers in slot order
+  enqueueExclusiveScan(c, keep, (size_t)n, pos);
+  enqueueExclusiveScan(c, aliveBySlot, (size_t)n, newSlot);
+  CK(cudaGetLastError());
+  k_compact<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, c->alt, keep, pos, newSlot, n);
+  uint32_t kept = 0, lastKeep = 0;
+  CK(cudaMemcpyAsync(&kept, pos + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&lastKeep, keep + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  if (hKeep) {
+    hKeep->resize(n);
+    CK(cudaMemcpyAsync(hKeep->data(), keep, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  std::swap(c->cur, c->alt);
+  c->n = (size_t)kept + lastKeep;
+  c->orderValid = false;
+  dropGraphs(c);
+  return LADDS_OK;
+}
+
 // Conjunction scan of the current state (cell keys, sort, gather, pair scan),
 // re-run with larger buffers after an overflow; sorted records in recs.
 int scanState(ladds_gpu_ctx *c, const ScanConsts &sc, float cutF, std::vector<ladds_pair> &recs) {
@@ -1457,33 +1486,86 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   const int n = (int)c->n;
   const double crit = kREarth + minAltitude;  // Simulation.cpp:573
   const double critSq = crit * crit;           // Simulation.cpp:581
-  uint32_t *keep = c->scratchA, *pos = c->scratchB, *aliveBySlot = c->scratchC, *newSlot = c->keys1;
-  k_burnup_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, c->cur.tag, n, critSq, keep,
-                                                        aliveBySlot);
-  // exclusive scans: positions in the current order, new slot numbers in slot order
-  enqueueExclusiveScan(c, keep, (size_t)n, pos);
-  enqueueExclusiveScan(c, aliveBySlot, (size_t)n, newSlot);
-  CK(cudaGetLastError());
-  k_compact<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, c->alt, keep, pos, newSlot, n);
-  CK(cudaStreamSynchronize(c->st));
-  CK(cudaGetLastError());
-  std::vector<uint32_t> hKeep(n);
-  CK(cudaMemcpy(hKeep.data(), keep, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  size_t kept = 0;
-  for (int i = 0; i < n; ++i) kept += hKeep[i];
-  const size_t removed = c->n - kept;
-  if (removedIds && removed) {
+  k_burnup_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, c->cur.tag, n, critSq,
+                                                        c->scratchA, c->scratchC);
+  std::vector<uint32_t> hKeep;
+  int rc = compactKept(c, &hKeep);
+  if (rc) return rc;
+  const size_t removed = (size_t)n - c->n;
+  if (removedIds && removed) {  // ids of the removed objects from the pre-compaction buffer
     std::vector<uint64_t> ids(n);
-    CK(cudaMemcpy(ids.data(), c->cur.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ids.data(), c->alt.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     size_t w = 0;
     for (int i = 0; i < n && w < cap; ++i)
       if (!hKeep[i]) removedIds[w++] = ids[i];
   }
-  std::swap(c->cur, c->alt);
-  c->n = kept;
   if (nRemoved) *nRemoved = removed;
-  c->orderValid = false;
-  dropGraphs(c);
+  return LADDS_OK;
+}
+
+int ladds_gpu_remove_slots(ladds_gpu_ctx *c, const uint32_t *slots, size_t m) {
+  if (!c || (m && !slots)) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (!m || !c->n) return LADDS_OK;
+  for (size_t i = 0; i < m; ++i)
+    if (slots[i] >= c->n) return fail(c, LADDS_ERR_INVALID_ARG, "slot out of range");
+  CK(cudaSetDevice(c->dev));
+  std::vector<uint8_t> mark(c->n, 0);
+  for (size_t i = 0; i < m; ++i) mark[slots[i]] = 1;
+  uint8_t *dMark = reinterpret_cast<uint8_t *>(c->scratchB);  // read before compactKept writes scratchB
+  CK(cudaMemcpyAsync(dMark, mark.data(), c->n, cudaMemcpyHostToDevice, c->st));
+  k_slot_mark_flags<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.tag, (int)c->n, dMark, c->scratchA,
+                                                              c->scratchC);
+  return compactKept(c, nullptr);
+}
+
+int ladds_gpu_select_layers(ladds_gpu_ctx *c, int32_t izLo, int32_t izHi, uint32_t *slots, size_t cap, size_t *n) {
+  if (!c || !n || (cap && !slots)) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  *n = 0;
+  if (!c->n || izHi <= izLo) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  unsigned *dCount = reinterpret_cast<unsigned *>(c->dCandNeed);  // scratch word (reset by every scan)
+  CK(cudaMemsetAsync(dCount, 0, sizeof(unsigned), c->st));
+  k_select_layers<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.z, c->cur.tag, (int)c->n, c->grid, izLo, izHi,
+                                                            c->scratchA, dCount, (unsigned)c->n);
+  unsigned cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, dCount, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  *n = cnt;
+  if (cnt > cap) return fail(c, LADDS_ERR_CAPACITY, "select_layers: buffer too small");
+  std::vector<uint32_t> h(cnt);
+  if (cnt) CK(cudaMemcpy(h.data(), c->scratchA, cnt * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  std::sort(h.begin(), h.end());
+  std::copy(h.begin(), h.end(), slots);
+  return LADDS_OK;
+}
+
+int ladds_gpu_layer_histogram(ladds_gpu_ctx *c, uint64_t *counts, size_t nLayers) {
+  if (!c || !counts) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  const size_t nz = (size_t)c->grid.n[2];
+  if (nLayers < nz) return fail(c, LADDS_ERR_CAPACITY, "layer_histogram: fewer entries than cell layers");
+  std::fill(counts, counts + nLayers, 0ull);
+  if (!c->n) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  if (nz > c->cap) return fail(c, LADDS_ERR_CAPACITY, "layer_histogram: more cell layers than capacity");
+  auto *dCounts = reinterpret_cast<unsigned long long *>(c->sortRec);  // cap entries of 8 B
+  CK(cudaMemsetAsync(dCounts, 0, nz * sizeof(unsigned long long), c->st));
+  k_layer_histogram<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.z, c->cur.tag, (int)c->n, c->grid, dCounts);
+  CK(cudaMemcpyAsync(counts, dCounts, nz * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  return LADDS_OK;
+}
+
+int ladds_gpu_set_halo(ladds_gpu_ctx *c, size_t haloStart) {
+  if (!c) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  const uint32_t h = haloStart >= (size_t)0xffffffffu ? 0xffffffffu : (uint32_t)haloStart;
+  if (h != c->haloStart) dropGraphs(c);  // captured scans carry the old value
+  c->haloStart = h;
   return LADDS_OK;
 }
 

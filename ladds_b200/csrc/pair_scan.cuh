@@ -130,6 +130,7 @@ struct CandSink {
   uint2 *cand;
   unsigned long long *count;
   unsigned long long half;
+  uint32_t haloStart;  // objects with slot >= haloStart are scan targets only, never sources
 };
 
 // Per-warp candidate buffer in shared memory with its fill count n held in a
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
   const int j = warpBase + lane;
   const bool inRange = j < n;
   const uint32_t myTag = inRange ? tags[j] : kTagDummy;
-  bool active = inRange && !tagDummy(myTag);
+  bool active = inRange && !tagDummy(myTag) && tagSlot(myTag) < out.haloStart;
   const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
   int32_t ix = 0, iy = 0, iz = 0;
   if (active) {
@@ -380,7 +381,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
       __syncwarp();
       for (uint32_t sBase = c0; sBase < c1; sBase += 32u) {
         const uint32_t si = sBase + (uint32_t)lane;
-        const bool src = si < c1 && !tagDummy(tags[si]);
+        const bool src = si < c1 && !tagDummy(tags[si]) && tagSlot(tags[si]) < out.haloStart;
         const float4 mf = src ? __ldg(&posf[si]) : make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t u = 0; u < m; ++u) {  // warp-uniform
           const float4 qq = sNb[warp][u];

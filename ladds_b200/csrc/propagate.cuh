@@ -112,6 +112,27 @@ __global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSt
   }
 }
 
+// slots of the live objects whose cell layer iz (the z index of the cell key)
+// lies in [lo, hi), appended in any order
+__global__ void k_select_layers(const double *__restrict__ z, const uint32_t *__restrict__ tag, int n, GridDesc g,
+                                int32_t lo, int32_t hi, uint32_t *__restrict__ out, unsigned *__restrict__ count,
+                                unsigned cap) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || tagDummy(tag[j])) return;
+  const int32_t iz = (int32_t)cellCoord(z[j], g.boxMin[2], g.invCell, g.n[2]);
+  if (iz < lo || iz >= hi) return;
+  const unsigned q = atomicAdd(count, 1u);
+  if (q < cap) out[q] = tagSlot(tag[j]);
+}
+
+// live objects per cell layer
+__global__ void k_layer_histogram(const double *__restrict__ z, const uint32_t *__restrict__ tag, int n, GridDesc g,
+                                  unsigned long long *__restrict__ counts) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || tagDummy(tag[j])) return;
+  atomicAdd(&counts[cellCoord(z[j], g.boxMin[2], g.invCell, g.n[2])], 1ull);
+}
+
 // Ephemeris of the stage times of `nSteps` steps starting at iteration `iter`
 // (one thread per stage), written to a global staging table that the host then
 // copies into c_eph.
