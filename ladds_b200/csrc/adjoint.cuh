@@ -243,13 +243,7 @@ __device__ __forceinline__ double pairMiss(const double ri[3], const double vi[3
   return dot3rn(dr, dr);
 }
 
-__device__ __forceinline__ void loadAtm(AtmShared &atm) {
-  for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
-    atm.h0[i] = c_atm[i].h0;
-    atm.rho0[i] = c_atm[i].rho0;
-    atm.H[i] = c_atm[i].H;
-  }
-}
+__device__ __forceinline__ void loadAtm(AtmShared &atm) { loadAtmTable(atm, c_atm); }
 
 __device__ __forceinline__ double shflPartner(unsigned m, double x) { return __shfl_xor_sync(m, x, 1); }
 

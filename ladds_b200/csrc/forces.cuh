@@ -12,7 +12,18 @@ namespace ladds {
 
 struct AtmShared {
   double h0[kAtmBands], rho0[kAtmBands], H[kAtmBands];
+  float invHf[kAtmBands];  // 1 / H in binary32 (split precision)
 };
+
+// stages the atmosphere table in shared memory (every thread of the block calls it)
+__device__ __forceinline__ void loadAtmTable(AtmShared &atm, const AtmRow *rows) {
+  for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
+    atm.h0[i] = rows[i].h0;
+    atm.rho0[i] = rows[i].rho0;
+    atm.H[i] = rows[i].H;
+    atm.invHf[i] = 1.0f / (float)rows[i].H;
+  }
+}
 
 // band index: largest k with h0[k] <= h (0 below the table)
 __device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
@@ -25,11 +36,14 @@ __device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
   return k;
 }
 
-// Battin's f(q) = (1+q)^{3/2} - 1 written without cancellation.
+// Battin's f(q) = (1+q)^{3/2} - 1 written without cancellation.  The
+// binary32 terms use the approximate square root (s * rsqrt(s)) and division
+// of the hardware: their few-ulp errors are far below the split form's
+// binary32 rounding of the perturbations themselves.
 __device__ __forceinline__ float battinF(float q) {
   const float s = 1.0f + q;
-  const float s32 = s * sqrtf(s);
-  return q * (3.0f + q * (3.0f + q)) / (1.0f + s32);
+  const float s32 = s * (s * rsqrtf(s));
+  return __fdividef(q * (3.0f + q * (3.0f + q)), 1.0f + s32);
 }
 
 template <bool SPLIT>
@@ -180,10 +194,11 @@ __device__ __forceinline__ void accel(uint32_t mask, const double r[3], const do
     if (mask & kPropDRAG) {
       const float wx = (float)v[0] + (float)kOmegaEarth * yf, wy = (float)v[1] - (float)kOmegaEarth * xf,
                   wz = (float)v[2];
-      const float wn = sqrtf(wx * wx + wy * wy + wz * wz);
+      const float w2 = wx * wx + wy * wy + wz * wz;
+      const float wn = w2 > 0.0f ? w2 * rsqrtf(w2) : 0.0f;
       const double h = rn - kREarth;
       const int b = atmBand(atm, h);
-      const float rho = (float)atm.rho0[b] * expf(-(float)(h - atm.h0[b]) / (float)atm.H[b]);
+      const float rho = (float)atm.rho0[b] * __expf(-(float)(h - atm.h0[b]) * atm.invHf[b]);
       const float k = -0.5e3f * rho * (float)bcInv * wn;
       bx += k * wx;
       by += k * wy;

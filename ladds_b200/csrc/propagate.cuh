@@ -50,11 +50,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate(DevState s, int n, int nSt
                                                    uint32_t *__restrict__ rowCount, uint32_t *__restrict__ arrival,
                                                    unsigned *__restrict__ status) {
   __shared__ AtmShared atm;
-  for (int i = threadIdx.x; i < kAtmBands; i += blockDim.x) {
-    atm.h0[i] = c_atm[i].h0;
-    atm.rho0[i] = c_atm[i].rho0;
-    atm.H[i] = c_atm[i].H;
-  }
+  loadAtmTable(atm, c_atm);
   __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (!KEYS && j >= n) return;
