@@ -12,7 +12,7 @@ namespace ladds {
 
 struct AtmShared {
   double h0[kAtmBands], rho0[kAtmBands], H[kAtmBands];
-  float invHf[kAtmBands];  // 1 / H in binary32 (split precision)
+  float h0f[kAtmBands], invHf[kAtmBands];  // h0 and 1 / H in binary32 (split precision)
 };
 
 // stages the atmosphere table in shared memory (every thread of the block calls it)
@@ -21,6 +21,7 @@ __device__ __forceinline__ void loadAtmTable(AtmShared &atm, const AtmRow *rows)
     atm.h0[i] = rows[i].h0;
     atm.rho0[i] = rows[i].rho0;
     atm.H[i] = rows[i].H;
+    atm.h0f[i] = (float)rows[i].h0;
     atm.invHf[i] = 1.0f / (float)rows[i].H;
   }
 }
@@ -32,6 +33,18 @@ __device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
   for (int step = 16; step >= 1; step >>= 1) {
     const int c = k + step;
     if (c < kAtmBands && h >= t.h0[c]) k = c;
+  }
+  return k;
+}
+// the same in binary32 (split precision: an altitude within binary32 rounding
+// of a band edge may take the neighbouring band, whose density agrees there to
+// the table's continuity)
+__device__ __forceinline__ int atmBandF(const AtmShared &t, float h) {
+  int k = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int c = k + step;
+    if (c < kAtmBands && h >= t.h0f[c]) k = c;
   }
   return k;
 }
@@ -196,9 +209,9 @@ __device__ __forceinline__ void accel(uint32_t mask, const double r[3], const do
                   wz = (float)v[2];
       const float w2 = wx * wx + wy * wy + wz * wz;
       const float wn = w2 > 0.0f ? w2 * rsqrtf(w2) : 0.0f;
-      const double h = rn - kREarth;
-      const int b = atmBand(atm, h);
-      const float rho = (float)atm.rho0[b] * __expf(-(float)(h - atm.h0[b]) * atm.invHf[b]);
+      const float h = (float)(rn - kREarth);
+      const int b = atmBandF(atm, h);
+      const float rho = (float)atm.rho0[b] * __expf(-(h - atm.h0f[b]) * atm.invHf[b]);
       const float k = -0.5e3f * rho * (float)bcInv * wn;
       bx += k * wx;
       by += k * wy;
