@@ -155,16 +155,19 @@ def algorithmic_units(n):
 
 def profiled_traffic(n):
     """DRAM bytes per launch of each phase's main kernel from the committed ncu
-    summary (1e6 objects), scaled to n objects."""
-    out = {}
+    summary (1e6 objects), scaled to n objects, and the same capture's issue
+    and DRAM utilisation (fractions) of that kernel."""
+    out, util = {}, {}
     try:
         for line in open(os.path.join(ROOT, "profiles", "dram_traffic_population0_1e6.txt")):
             if line.strip() and not line.startswith("#"):
-                phase, _, nbytes = line.split()
-                out[phase] = int(nbytes) * n / 1e6
+                f = line.split()
+                out[f[0]] = int(f[2]) * n / 1e6
+                if len(f) >= 5:
+                    util[f[0]] = {"issue_active": float(f[3]) / 100.0, "dram_throughput": float(f[4]) / 100.0}
     except (OSError, ValueError):
         pass
-    return out
+    return out, util
 
 
 def propagation_flops(mask_full=True):
@@ -521,12 +524,19 @@ def main():
     if f64_peak:
         kernels["propagate_fp64_mode"]["fp64_frac"] = kernels["propagate_fp64_mode"]["achieved_tflops"] / f64_peak
     dk = kernels[dominant]
-    traffic = profiled_traffic(n).get(dominant)
+    traffic_all, util = profiled_traffic(n)
+    traffic = traffic_all.get(dominant)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["achieved_gbs"], "peak": hbm_peak,
                 "unit": "GB/s", "frac": dk["hbm_frac"], "traffic": traffic,
                 "traffic_source": "profiles/dram_traffic_population0_1e6.txt (one ncu capture, scaled by n/1e6)"
                 if traffic else None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback"}
+    if dominant in util:  # what the same ncu capture shows bounds the kernel instead of HBM
+        u = util[dominant]
+        roofline["ncu_issue_active"] = u["issue_active"]
+        roofline["ncu_dram_throughput"] = u["dram_throughput"]
+        roofline["limiter"] = ("instruction issue" if u["issue_active"] > 0.6 and u["dram_throughput"] < 0.3
+                               else "hbm" if u["dram_throughput"] > 0.5 else "latency")
 
     cpu = None
     if not args.no_cpu and world == 1:
