@@ -135,7 +135,8 @@ def dist_barrier(world):
 
 # ----------------------------------------------------------- algorithmic work
 def algorithmic_units(n):
-    """Per-step algorithmic bytes and flops of each phase (definitions in DESIGN.md)."""
+    """Per-step algorithmic bytes of each phase: the bytes the phase must move per object
+    at the least, from the data each kernel reads and writes (listed per entry)."""
     return {
         # read r, v, aom, bcInv, tag (68 B), write r, v (48 B), write the cell key (4 B)
         "propagate": {"bytes": n * 120},
@@ -171,7 +172,9 @@ def profiled_traffic(n):
 
 
 def propagation_flops(mask_full=True):
-    # counted FP operations per force evaluation of the restated model
+    # counted FP operations per force evaluation of the restated model (transcendentals as 1):
+    # radius terms 8, Kepler 8, J2 18, J3 25, C22/S22 42, Sun 24, Moon 24, SRP 28, drag 28 + band
+    # search = 208; Kepler + J2 alone 33; + 42 for the drift / kick updates of a step
     f_eval = 208 if mask_full else 33
     return 3 * f_eval + 42
 
