@@ -13,8 +13,10 @@ figure, their ratio and the one-day RMS drift of split vs FP64 are reported
 beside it.  ``e2e`` runs the same steps through the C ABI in the host-owned
 mode of the drop-in: per step the positions/velocities go host->device from
 pinned memory, the step runs, positions/velocities and the conjunction
-records come back.  ``--impl reference`` times the CPU restatement of the
-reference path (the oracle; the reference itself cannot be built here).
+records come back; ``e2e.device_resident`` is the drop-in's own data flow, the
+population kept on the device and each iteration's records read back.
+``--impl reference`` times the CPU restatement of the reference path (the
+oracle; the reference itself cannot be built here).
 """
 from __future__ import annotations
 
@@ -490,6 +492,21 @@ def main():
         e2e = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": int(48 * n + rec_bytes / args.e2e_steps),
                "steps": args.e2e_steps, "mode": "host-owned state (set_state / step(1) / get_state, pinned)"}
+        # the drop-in's own data flow (ladds::HotPathLoop): the population stays on the device and
+        # each iteration's records come back to the host (pinned) from one ladds_gpu_step(1) call
+        outp = torch.empty((1 << 16) * capi.PAIR_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True).numpy()
+        outp = outp.view(capi.PAIR_DTYPE)
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        rec_bytes = 0
+        for _ in range(args.e2e_steps):
+            r = ctx.step(1, out=outp)
+            rec_bytes += len(r.records) * 64 + 8
+        el = dist_max(time.perf_counter() - t0, world)
+        e2e["device_resident"] = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
+                                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(rec_bytes / args.e2e_steps),
+                                  "mode": "device-resident population, records to pinned host memory "
+                                          "(ladds_gpu_step(1) per iteration)"}
         ctx.close()
     except Exception as ex:  # noqa: BLE001
         e2e = {"value": None, "unit": "object-steps/s", "error": str(ex)[:200]}

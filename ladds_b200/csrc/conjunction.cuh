@@ -268,16 +268,22 @@ __global__ void k_mark_deleted(uint32_t *__restrict__ tag, const uint8_t *__rest
 }
 
 // keep[j] = 1 if the object survives the burn-up test |r|^2 >= crit^2
-// (Simulation.cpp:581-590); aliveBySlot[slot] mirrors it in slot order.
+// (Simulation.cpp:581-590); aliveBySlot[slot] mirrors it in slot order;
+// *burnt counts the objects that fail it (one atomic per warp that has any).
 __global__ void k_burnup_flags(const double *__restrict__ x, const double *__restrict__ y,
                                const double *__restrict__ z, const uint32_t *__restrict__ tag, int n,
-                               double critSq, uint32_t *__restrict__ keep, uint32_t *__restrict__ aliveBySlot) {
+                               double critSq, uint32_t *__restrict__ keep, uint32_t *__restrict__ aliveBySlot,
+                               unsigned *__restrict__ burnt) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const double a2 = x[j] * x[j] + y[j] * y[j] + z[j] * z[j];
-  const uint32_t k = (a2 < critSq) ? 0u : 1u;
-  keep[j] = k;
-  if (tagSlot(tag[j]) < (uint32_t)n) aliveBySlot[tagSlot(tag[j])] = k;
+  uint32_t k = 1u;
+  if (j < n) {
+    const double a2 = x[j] * x[j] + y[j] * y[j] + z[j] * z[j];
+    k = (a2 < critSq) ? 0u : 1u;
+    keep[j] = k;
+    if (tagSlot(tag[j]) < (uint32_t)n) aliveBySlot[tagSlot(tag[j])] = k;
+  }
+  const unsigned below = __ballot_sync(0xffffffffu, k == 0u);
+  if (below && (threadIdx.x & 31) == 0) atomicAdd(burnt, (unsigned)__popc(below));
 }
 
 // keep[j] = 0 for the objects whose slot is marked (slotMark[slot] = 1);

@@ -1486,8 +1486,15 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   const int n = (int)c->n;
   const double crit = kREarth + minAltitude;  // Simulation.cpp:573
   const double critSq = crit * crit;           // Simulation.cpp:581
+  unsigned *dBurnt = reinterpret_cast<unsigned *>(c->dCandNeed);  // scratch word (reset by every scan)
+  CK(cudaMemsetAsync(dBurnt, 0, sizeof(unsigned), c->st));
   k_burnup_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur.x, c->cur.y, c->cur.z, c->cur.tag, n, critSq,
-                                                        c->scratchA, c->scratchC);
+                                                        c->scratchA, c->scratchC, dBurnt);
+  unsigned burnt = 0;
+  CK(cudaMemcpyAsync(&burnt, dBurnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  if (!burnt) return LADDS_OK;  // nothing burns up: the state, its order and the captured graphs stay
   std::vector<uint32_t> hKeep;
   int rc = compactKept(c, &hKeep);
   if (rc) return rc;
