@@ -167,6 +167,18 @@ cudaError_t allocState(DevState &s, size_t cap) {
   return e;
 }
 
+// positions and velocities only
+cudaError_t copyDynamic(const DevState &src, const DevState &dst, size_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz};
+  double *dd[] = {dst.x, dst.y, dst.z, dst.vx, dst.vy, dst.vz};
+  for (int k = 0; k < 6; ++k) {
+    cudaError_t e = cudaMemcpyAsync(dd[k], sd[k], n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t copyState(const DevState &src, const DevState &dst, size_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.aom, src.bc, src.radius};
@@ -628,6 +640,30 @@ int syncAndStatus(ladds_gpu_ctx *c) {
   return LADDS_OK;
 }
 
+// syncAndStatus + growIfOverflowed with one read of the three words after the sync
+int syncStatusAndGrow(ladds_gpu_ctx *c, unsigned long long *records, bool *overflow) {
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  unsigned long long w[3] = {0, 0, 0};  // record count, largest candidate count, status
+  CK(cudaMemcpy(w, c->dCount, sizeof(w), cudaMemcpyDeviceToHost));
+  const unsigned status = (unsigned)(w[2] & 0xffffffffull);
+  if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
+  if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
+  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait gave up (sort look-back)");
+  if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
+  *records = w[0];
+  *overflow = w[0] > c->pairCap || w[1] > c->candCap;
+  if (w[0] > c->pairCap) {
+    const int rc = ensurePairCapacity(c, (size_t)w[0]);
+    if (rc) return rc;
+  }
+  if (w[1] > c->candCap) {
+    const int rc = ensureCandCapacity(c, (size_t)w[1]);
+    if (rc) return rc;
+  }
+  return LADDS_OK;
+}
+
 bool pairLess(const ladds_pair &a, const ladds_pair &b) {
   if (a.step != b.step) return a.step < b.step;
   if (a.idA != b.idA) return a.idA < b.idA;
@@ -820,10 +856,8 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       allocGridBuffers(c) != LADDS_OK || cudaMalloc(&c->longCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->denseCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->denseCountB, sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->dCount, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dCount, 3 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dCandCount, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&c->dCandNeed, sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&c->dStatus, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
       cudaMalloc(&c->dIter, 2 * sizeof(int64_t)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess) {
@@ -832,7 +866,10 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
     return LADDS_ERR_ALLOC;
   }
   c->dIterBase = c->dIter + 1;
-  cudaMemset(c->dStatus, 0, sizeof(unsigned));
+  // record count, largest candidate count and status words side by side: one read after a step
+  c->dCandNeed = c->dCount + 1;
+  c->dStatus = reinterpret_cast<unsigned *>(c->dCount + 2);
+  cudaMemset(c->dCount, 0, 3 * sizeof(unsigned long long));
   cudaMemset(c->dCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dIter, 0, 2 * sizeof(int64_t));
   cudaEventCreate(&c->callStart);
@@ -865,8 +902,8 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   freeBuffers(c);
   freeGridBuffers(c);
   void *ptrs[] = {c->longCount, c->denseCount, c->denseCells, c->denseCountB, c->denseCellsB, c->dCount,
-                  c->dStatus, c->dEph,
-                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dCandNeed, c->dObj,
+                  c->dEph,
+                  c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dObj,
                   c->adj.st, c->adj.bc, c->adj.aom, c->adj.miss, c->adj.grad, c->adj.ckpt, c->adj.rec,
                   c->adj.off, c->adj.arg, c->adj.eph};
   for (void *p : ptrs)
@@ -1302,11 +1339,26 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
   int scans = 0;
   for (int i = 0; i < iterations; ++i) scans += ((c->hostIter + i) % k) == 0;
   // snapshot of the call's start state: the call is re-run after a device
-  // pair-buffer overflow and undone when the caller's buffer is too small
-  CK(copyState(c->cur, c->snap, c->n, c->st));
+  // pair-buffer overflow and undone when the caller's buffer is too small.  A
+  // one-iteration call changes only the positions and velocities of the
+  // current buffer (its gather writes the other buffer), so they are all it
+  // keeps; undoing it restores them and the buffer roles.
+  const bool light = iterations == 1;
+  const DevState curStart = c->cur, altStart = c->alt;
+  if (light) {
+    CK(copyDynamic(c->cur, c->snap, c->n, c->st));
+  } else {
+    CK(copyState(c->cur, c->snap, c->n, c->st));
+  }
   const int64_t startIter = c->hostIter;
   auto rollBack = [&]() -> int {
-    CK(copyState(c->snap, c->cur, c->n, c->st));
+    if (light) {
+      c->cur = curStart;
+      c->alt = altStart;
+      CK(copyDynamic(c->snap, c->cur, c->n, c->st));
+    } else {
+      CK(copyState(c->snap, c->cur, c->n, c->st));
+    }
     CK(cudaMemcpyAsync(c->dIter, &startIter, sizeof(int64_t), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
     c->hostIter = startIter;
@@ -1318,7 +1370,7 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
   for (;;) {
     CK(cudaMemsetAsync(c->dCount, 0, sizeof(unsigned long long), c->st));
     CK(cudaMemsetAsync(c->dCandNeed, 0, sizeof(unsigned long long), c->st));
-    const bool graph = c->cfg.useGraphs && !c->profiling && iterations > 1;
+    const bool graph = c->cfg.useGraphs && !c->profiling && iterations >= 1;
     const int64_t it0 = c->hostIter;
     if (graph) {
       // pass 1: capture the graphs this call needs (capture performs the host-side
@@ -1372,17 +1424,12 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       }
     }
     CK(cudaEventRecord(c->callEnd, c->st));
-    int rc = syncAndStatus(c);
+    bool overflow = false;
+    int rc = syncStatusAndGrow(c, &cnt, &overflow);
     collectTimes(c);
     if (rc) {
       const int rb = rollBack();
       return rb ? rb : rc;
-    }
-    bool overflow = false;
-    rc = growIfOverflowed(c, &cnt, &overflow);
-    if (rc) {
-      rollBack();
-      return rc;
     }
     if (!overflow) break;
     // a device record or candidate buffer overflowed: it has grown; roll back, run the batch again
