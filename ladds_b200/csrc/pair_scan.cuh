@@ -274,15 +274,44 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
     }
   }
   const double c2 = g.cellSize * g.cellSize;
+  // Dense populations (the buffer form) with cells below the cutoff (reach >=
+  // 2): the object's own x-window in
+  // each neighbour row: partners lie within reachF of it, and a row whose
+  // (y, z) cell box is dyMin, dzMin away can hold them only within
+  // hw = sqrt(reachF^2 - dyMin^2 - dzMin^2) of its x.  Binary32 geometry with a
+  // 50 m margin over the pre-filter radius (which dwarfs the rounding of
+  // positions and cell edges); offsets inside the own cell are clamped to the
+  // cell, which only widens the windows of objects clamped into boundary
+  // cells.  With reach 1, or sparse populations (the list form), the cell
+  // windows are kept: trimming them does not pay for its arithmetic.
+  const bool perObject = SCREEN == LADDS_SCREEN_BUFFER && R >= 2;  // warp-uniform
+  const float4 me = active && perObject ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float cf = (float)g.cellSize, invCf = (float)g.invCell;
+  const float fy = fminf(fmaxf(me.y - ((float)g.boxMin[1] + (float)iy * cf), 0.f), cf);
+  const float fz = fminf(fmaxf(me.z - ((float)g.boxMin[2] + (float)iz * cf), 0.f), cf);
+  const float xRel = me.x - (float)g.boxMin[0];
+  const float reachF = cutF + 0.05f, reachF2 = reachF * reachF;
   for (int dz = 0; dz <= R; ++dz) {
+    const float dzMin = dz == 0 ? 0.f : (float)(dz - 1) * cf + (cf - fz);
     for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
       const int w = rowHalfWidth(dy, dz, R, c2, reachR2);  // warp-uniform
       if (w < 0) continue;
       const int32_t jz = iz + dz, jy = iy + dy;
-      const bool ok = active && jz < nz && jy >= 0 && jy < ny;
+      int32_t lo32 = dz == 0 && dy == 0 ? ix : max(ix - w, 0), hi32 = min(ix + w, nx - 1);
+      bool inReach = true;
+      if (perObject) {
+        const float dyMin =
+            dy == 0 ? 0.f : dy > 0 ? (float)(dy - 1) * cf + (cf - fy) : (float)(-dy - 1) * cf + fy;
+        const float h2 = reachF2 - dyMin * dyMin - dzMin * dzMin;
+        const float hw = h2 > 0.f ? h2 * rsqrtf(h2) : 0.f;
+        if (!(dz == 0 && dy == 0)) lo32 = max(lo32, (int32_t)floorf((xRel - hw) * invCf));
+        hi32 = min(hi32, (int32_t)floorf((xRel + hw) * invCf));
+        inReach = h2 >= 0.f && hi32 >= lo32;
+      }
+      const bool ok = active && jz < nz && jy >= 0 && jy < ny && inReach;
       const uint32_t r2 = ok ? (uint32_t)jz * (uint32_t)ny + (uint32_t)jy : 0u;
-      const uint32_t xlo = ok ? (dz == 0 && dy == 0 ? (uint32_t)ix : (uint32_t)max(ix - w, 0)) : 0u;
-      const uint32_t xhi = ok ? (uint32_t)min(ix + w, nx - 1) : 0u;
+      const uint32_t xlo = ok ? (uint32_t)lo32 : 0u;
+      const uint32_t xhi = ok ? (uint32_t)hi32 : 0u;
       const RowLookup L = rowLoads(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff);  // four reads in flight
       uint32_t lo = 0, hi = 0;
       if (ok) {
