@@ -635,7 +635,6 @@ int syncAndStatus(ladds_gpu_ctx *c) {
   CK(cudaMemcpy(&status, c->dStatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
   if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
-  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait gave up (sort look-back)");
   if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
   return LADDS_OK;
 }
@@ -649,7 +648,6 @@ int syncStatusAndGrow(ladds_gpu_ctx *c, unsigned long long *records, bool *overf
   const unsigned status = (unsigned)(w[2] & 0xffffffffull);
   if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
   if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
-  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait gave up (sort look-back)");
   if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
   *records = w[0];
   *overflow = w[0] > c->pairCap || w[1] > c->candCap;
