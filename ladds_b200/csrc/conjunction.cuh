@@ -176,22 +176,31 @@ __device__ __forceinline__ uint32_t functorPair(const ScanConsts &c, const Obj &
 //   positions: per-coordinate rounding <= posf.w (a 4x bound), velocities
 //   2^-24 |v| per coordinate, times dt; the closest approach over t is
 //   1-Lipschitz in the separation and dt-Lipschitz in the relative velocity;
-//   binary32 arithmetic on separations of size S: 2^-20 S.
+//   binary32 arithmetic on separations of size S: 2^-20 S.  FAST: the division
+//   and the square roots are the hardware approximations (relative errors of
+//   a few 2^-23): an error in t moves the distance at second order, and the
+//   distances' own relative error stays far inside the 1e-6 S term.  (FAST
+//   pays where the screen dominates -- dense populations -- and costs where it
+//   does not: its special-function work competes with the propagation that
+//   runs beside the scan.)
 // NaN (identical velocities: the reference's 0/0 path) keeps the pair.
+template <bool FAST = false>
 __device__ __forceinline__ bool mayRecord(const ScanConsts &c, float4 pa, float4 va, float4 pb, float4 vb) {
   const float dt = (float)c.dt;
   const float drx = pa.x - pb.x, dry = pa.y - pb.y, drz = pa.z - pb.z;
   const float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
   const float ox = drx - dvx * dt, oy = dry - dvy * dt, oz = drz - dvz * dt;  // separation at the step start
   const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
-  float t = -(ox * dvx + oy * dvy + oz * dvz) / dv2;
+  const float num = -(ox * dvx + oy * dvy + oz * dvz);
+  float t = FAST ? __fdividef(num, dv2) : num / dv2;  // 0/0: NaN, kept below
   t = (t < 0.0f) ? 0.0f : ((dt < t) ? dt : t);
   const float mx = ox + dvx * t, my = oy + dvy * t, mz = oz + dvz * t;
-  const float dl = sqrtf(mx * mx + my * my + mz * mz);
+  const float m2 = mx * mx + my * my + mz * mz;
+  const float dl = FAST ? m2 * rsqrtf(m2) : sqrtf(m2);  // FAST: 0 * inf = NaN for m2 = 0, kept
   const float d2 = drx * drx + dry * dry + drz * drz;
   const float vmax = fmaxf(fmaxf(fabsf(va.x), fabsf(va.y)), fabsf(va.z)) +
                      fmaxf(fmaxf(fabsf(vb.x), fabsf(vb.y)), fabsf(vb.z));
-  const float sepScale = sqrtf(d2) + sqrtf(dv2) * dt;
+  const float sepScale = FAST ? d2 * rsqrtf(d2) + dv2 * rsqrtf(dv2) * dt : sqrtf(d2) + sqrtf(dv2) * dt;
   const float err = 3.5f * (pa.w + pb.w) + 3.5e-7f * vmax * dt + 1e-6f * sepScale + 1e-6f;
   const float rel = 1.0f + 4.0f * (float)c.nearRel + 1e-6f;
   const float sep = (va.w + vb.w) * (float)c.factor;

@@ -158,6 +158,7 @@ __device__ __forceinline__ void warpSpill(int lane, uint2 *buf, uint32_t &n, con
 // full): screened 32 pairs at a time (all four loads of a lane in flight
 // together); the survivors are appended to the screened list with one global
 // atomic per round that has any.
+template <int SCREEN>
 __device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, const CandSink &out) {
   __syncwarp();
   for (uint32_t b = 0; b < n; b += 32u) {
@@ -166,7 +167,7 @@ __device__ __forceinline__ void warpFlush(int lane, uint2 *buf, uint32_t &n, con
     bool keep = false;
     if (i < n) {
       p = buf[i];
-      keep = mayRecord(out.sc, __ldg(&out.posf[p.x]), __ldg(&out.velf[p.x]), __ldg(&out.posf[p.y]),
+      keep = mayRecord<SCREEN == LADDS_SCREEN_BUFFER>(out.sc, __ldg(&out.posf[p.x]), __ldg(&out.velf[p.x]), __ldg(&out.posf[p.y]),
                        __ldg(&out.velf[p.y]));
     }
     const uint32_t mask = __ballot_sync(0xffffffffu, keep);
@@ -189,7 +190,7 @@ __device__ __forceinline__ void warpAppend(bool pass, uint32_t j, uint32_t k, in
   if (!mask) return;
   if (n + (uint32_t)__popc(mask) > (uint32_t)kWarpCand) {
     if (SCREEN == LADDS_SCREEN_BUFFER)
-      warpFlush(lane, buf, n, out);
+      warpFlush<SCREEN>(lane, buf, n, out);
     else
       warpSpill(lane, buf, n, out);
   }
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
       warpWindowPairs<SCREEN>(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
     }
   }
-  warpFlush(lane, sCand[warp], nBuf, out);
+  warpFlush<SCREEN>(lane, sCand[warp], nBuf, out);
 }
 
 // Dense bin of the pair scan (cells with >= kDenseCell objects, listed by the
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
       __syncwarp();
     }
   }
-  warpFlush(lane, sCand[warp], nBuf, out);
+  warpFlush<SCREEN>(lane, sCand[warp], nBuf, out);
 }
 
 
