@@ -146,8 +146,9 @@ def algorithmic_units(n):
         "bucket": {"bytes": n * (4 + 8 + 12)},
         # row sort: record + source in (12), sorted key + slot out (8)
         "rowsort": {"bytes": n * (12 + 8)},
-        # gather 92 B + perm 4 into cell order; write 92 B SoA + 32 B binary32 position / velocity copies
-        "permute": {"bytes": n * (92 + 4 + 92 + 32)},
+        # gather r, v, aom, bcInv, tag (68 B) + perm 4 into cell order, radius by slot (8 B); write 68 B SoA
+        # + 32 B binary32 position / velocity copies (radius, id, parent stay in slot order)
+        "permute": {"bytes": n * (68 + 4 + 8 + 68 + 32)},
         # own key, tag, posf (24 B) + the closest-approach screen of the pre-filtered pairs: binary32
         # position + velocity of both objects (64 B, ~1.5 pairs per object)
         "candidates": {"bytes": n * (24 + 96)},

@@ -51,9 +51,8 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   }
   const double x = src.x[p], y = src.y[p], z = src.z[p];
   const double vx = src.vx[p], vy = src.vy[p], vz = src.vz[p];
-  const double radius = src.radius[p];
-  const uint64_t id = src.id[p], parent = src.parent[p];
   const uint32_t tag = src.tag[p];
+  const double radius = tagSlot(tag) < (uint32_t)n ? src.radius[tagSlot(tag)] : 0.0;  // slot-indexed
   dst.x[j] = x;
   dst.y[j] = y;
   dst.z[j] = z;
@@ -62,9 +61,6 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   dst.vz[j] = vz;
   dst.aom[j] = src.aom[p];
   dst.bc[j] = src.bc[p];
-  dst.radius[j] = radius;
-  dst.id[j] = id;
-  dst.parent[j] = parent;
   dst.tag[j] = tag;
   pk.posf[j] = floatPosition(x, y, z);
   pk.velf[j] = make_float4((float)vx, (float)vy, (float)vz, __double2float_ru(radius));
@@ -111,31 +107,20 @@ struct Obj {
   uint32_t tag;
 };
 
+// (positions by the pre-gather position perm[k], radius / id / parent by slot)
 __device__ __forceinline__ void loadObjPacked(const ScanPack &pk, uint32_t k, Obj &o) {
   const uint32_t p = pk.perm[k];
   o.r[0] = pk.src.x[p];
   o.r[1] = pk.src.y[p];
   o.r[2] = pk.src.z[p];
-  o.radius = pk.src.radius[p];
   o.v[0] = pk.src.vx[p];
   o.v[1] = pk.src.vy[p];
   o.v[2] = pk.src.vz[p];
-  o.id = pk.src.id[p];
-  o.parent = pk.src.parent[p];
   o.tag = pk.src.tag[p];
-}
-
-__device__ __forceinline__ void loadObj(const DevState &s, int k, Obj &o) {
-  o.r[0] = s.x[k];
-  o.r[1] = s.y[k];
-  o.r[2] = s.z[k];
-  o.v[0] = s.vx[k];
-  o.v[1] = s.vy[k];
-  o.v[2] = s.vz[k];
-  o.radius = s.radius[k];
-  o.id = s.id[k];
-  o.parent = s.parent[k];
-  o.tag = s.tag[k];
+  const uint32_t s = tagSlot(o.tag);
+  o.radius = pk.src.radius[s];
+  o.id = pk.src.id[s];
+  o.parent = pk.src.parent[s];
 }
 
 // CollisionFunctor::AoSFunctor on (i, j) with the gate already evaluated.
@@ -249,11 +234,6 @@ __global__ void k_unpermute_f64(const double *__restrict__ src, const uint32_t *
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = src[j];
 }
-__global__ void k_unpermute_u64(const uint64_t *__restrict__ src, const uint32_t *__restrict__ tag, int n,
-                                uint64_t *__restrict__ dst) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = src[j];
-}
 __global__ void k_unpermute_act(const uint32_t *__restrict__ tag, int n, int8_t *__restrict__ dst) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = (int8_t)tagAct(tag[j]);
@@ -307,9 +287,12 @@ __global__ void k_slot_mark_flags(const uint32_t *__restrict__ tag, int n, const
   if (s < (uint32_t)n) aliveBySlot[s] = k;
 }
 
-// compaction: dst[pos[j]] = src[j] for kept j; slots renumbered via newSlot
+// compaction: dst[pos[j]] = src[j] for kept j, slots renumbered via newSlot;
+// the slot-indexed arrays go to the new slots of separate arrays (tRadius,
+// tId, tParent), as the state buffers share theirs
 __global__ void k_compact(DevState src, DevState dst, const uint32_t *__restrict__ keep,
-                          const uint32_t *__restrict__ pos, const uint32_t *__restrict__ newSlot, int n) {
+                          const uint32_t *__restrict__ pos, const uint32_t *__restrict__ newSlot, int n,
+                          double *__restrict__ tRadius, uint64_t *__restrict__ tId, uint64_t *__restrict__ tParent) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n || !keep[j]) return;
   const uint32_t p = pos[j];
@@ -321,12 +304,13 @@ __global__ void k_compact(DevState src, DevState dst, const uint32_t *__restrict
   dst.vz[p] = src.vz[j];
   dst.aom[p] = src.aom[j];
   dst.bc[p] = src.bc[j];
-  dst.radius[p] = src.radius[j];
-  dst.id[p] = src.id[j];
-  dst.parent[p] = src.parent[j];
-  const uint32_t t = src.tag[j];
-  const uint32_t ns = tagSlot(t) < (uint32_t)n ? newSlot[tagSlot(t)] : 0u;
+  const uint32_t t = src.tag[j], s = tagSlot(t);
+  if (s >= (uint32_t)n) return;  // only with a corrupted tag
+  const uint32_t ns = newSlot[s];
   dst.tag[p] = (t & ~kTagSlotMask) | (ns & kTagSlotMask);
+  tRadius[ns] = src.radius[s];
+  tId[ns] = src.id[s];
+  tParent[ns] = src.parent[s];
 }
 
 // exclusive scan of u32 flags, three phases (block sums, scan of sums, apply)

@@ -88,11 +88,12 @@ __global__ void k_gather_records(DevState s, const int32_t *__restrict__ pos, in
   r.v[0] = s.vx[j];
   r.v[1] = s.vy[j];
   r.v[2] = s.vz[j];
-  r.radius = s.radius[j];
+  const uint32_t slot = tagSlot(s.tag[j]);  // radius, id and parent are indexed by slot
+  r.radius = s.radius[slot];
   r.aom = s.aom[j];
   r.bcInv = s.bc[j];
-  r.id = s.id[j];
-  r.parentId = s.parent[j];
+  r.id = s.id[slot];
+  r.parentId = s.parent[slot];
   r.activity = tagAct(s.tag[j]);
   r.deleted = tagDummy(s.tag[j]) ? 1u : 0u;
   out[q] = r;

@@ -147,23 +147,40 @@ int fail(ladds_gpu_ctx *c, int code, const std::string &msg) {
       return fail(c, LADDS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
   } while (0)
 
-void freeState(DevState &s) {
-  void *ptrs[] = {s.x, s.y, s.z, s.vx, s.vy, s.vz, s.aom, s.bc, s.radius, s.id, s.parent, s.tag};
+// frees a state buffer; the slot-indexed arrays (radius, id, parent) only
+// when withSlotArrays (a context's buffers share them)
+void freeState(DevState &s, bool withSlotArrays) {
+  void *ptrs[] = {s.x, s.y, s.z, s.vx, s.vy, s.vz, s.aom, s.bc, s.tag};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (withSlotArrays) {
+    void *shared[] = {s.radius, s.id, s.parent};
+    for (void *p : shared)
+      if (p) cudaFree(p);
+  }
   s = DevState{};
 }
 
-cudaError_t allocState(DevState &s, size_t cap) {
+// allocates a state buffer; the slot-indexed arrays are taken from `shared`
+// (or allocated when it has none)
+cudaError_t allocState(DevState &s, size_t cap, const DevState *shared) {
   s = DevState{};
-  double **d[] = {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.aom, &s.bc, &s.radius};
+  double **d[] = {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.aom, &s.bc};
   for (double **p : d) {
     cudaError_t e = cudaMalloc(p, cap * sizeof(double));
     if (e != cudaSuccess) return e;
   }
-  cudaError_t e = cudaMalloc(&s.id, cap * sizeof(uint64_t));
+  cudaError_t e = cudaMalloc(&s.tag, cap * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  if (shared) {
+    s.radius = shared->radius;
+    s.id = shared->id;
+    s.parent = shared->parent;
+    return cudaSuccess;
+  }
+  e = cudaMalloc(&s.radius, cap * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&s.id, cap * sizeof(uint64_t));
   if (e == cudaSuccess) e = cudaMalloc(&s.parent, cap * sizeof(uint64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&s.tag, cap * sizeof(uint32_t));
   return e;
 }
 
@@ -179,17 +196,20 @@ cudaError_t copyDynamic(const DevState &src, const DevState &dst, size_t n, cuda
   return cudaSuccess;
 }
 
+// copies a state buffer (the slot-indexed arrays only when the buffers do not share them)
 cudaError_t copyState(const DevState &src, const DevState &dst, size_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.aom, src.bc, src.radius};
-  double *dd[] = {dst.x, dst.y, dst.z, dst.vx, dst.vy, dst.vz, dst.aom, dst.bc, dst.radius};
-  for (int k = 0; k < 9; ++k) {
+  const double *sd[] = {src.x, src.y, src.z, src.vx, src.vy, src.vz, src.aom, src.bc};
+  double *dd[] = {dst.x, dst.y, dst.z, dst.vx, dst.vy, dst.vz, dst.aom, dst.bc};
+  for (int k = 0; k < 8; ++k) {
     cudaError_t e = cudaMemcpyAsync(dd[k], sd[k], n * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return e;
   }
-  cudaError_t e = cudaMemcpyAsync(dst.id, src.id, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(dst.tag, src.tag, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess || src.id == dst.id) return e;
+  e = cudaMemcpyAsync(dst.radius, src.radius, n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst.id, src.id, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dst.parent, src.parent, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dst.tag, src.tag, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
   return e;
 }
 
@@ -201,9 +221,9 @@ void dropGraphs(ladds_gpu_ctx *c) {
 int ensureCandCapacity(ladds_gpu_ctx *c, size_t need);
 
 void freeBuffers(ladds_gpu_ctx *c) {
-  freeState(c->cur);
-  freeState(c->alt);
-  freeState(c->snap);
+  freeState(c->cur, true);
+  freeState(c->alt, false);
+  freeState(c->snap, false);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
                   c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf, c->keys1B, c->vals1B};
   for (void *p : ptrs)
@@ -224,13 +244,13 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   size_t newCap = std::max<size_t>({need, c->cap + c->cap / 2, 4096});
   newCap = std::min(newCap, kMaxObjects);
   DevState ncur, nalt, nsnap;
-  cudaError_t e = allocState(ncur, newCap);
-  if (e == cudaSuccess) e = allocState(nalt, newCap);
-  if (e == cudaSuccess) e = allocState(nsnap, newCap);
+  cudaError_t e = allocState(ncur, newCap, nullptr);
+  if (e == cudaSuccess) e = allocState(nalt, newCap, &ncur);
+  if (e == cudaSuccess) e = allocState(nsnap, newCap, &ncur);
   if (e != cudaSuccess) {
-    freeState(ncur);
-    freeState(nalt);
-    freeState(nsnap);
+    freeState(ncur, true);
+    freeState(nalt, false);
+    freeState(nsnap, false);
     cudaGetLastError();
     return fail(c, LADDS_ERR_ALLOC, std::string("device allocation failed: ") + cudaGetErrorString(e));
   }
@@ -1087,23 +1107,20 @@ int ladds_gpu_download(ladds_gpu_ctx *c, size_t cap, size_t *nOut, double *x, do
   if (!c->n) return LADDS_OK;
   CK(cudaSetDevice(c->dev));
   const int g = blocksFor(c->n, 256);
-  const double *src[] = {c->cur.x, c->cur.y, c->cur.z, c->cur.vx, c->cur.vy, c->cur.vz, c->cur.radius, c->cur.aom,
-                         c->cur.bc};
-  double *dst[] = {x, y, z, vx, vy, vz, radius, aom, bcInv};
-  for (int k = 0; k < 9; ++k) {
+  const double *src[] = {c->cur.x, c->cur.y, c->cur.z, c->cur.vx, c->cur.vy, c->cur.vz, c->cur.aom, c->cur.bc};
+  double *dst[] = {x, y, z, vx, vy, vz, aom, bcInv};
+  for (int k = 0; k < 8; ++k) {
     if (!dst[k]) continue;
     k_unpermute_f64<<<g, 256, 0, c->st>>>(src[k], c->cur.tag, (int)c->n, c->alt.x);
     CK(cudaMemcpyAsync(dst[k], c->alt.x, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
   }
-  const uint64_t *usrc[] = {c->cur.id, c->cur.parent};
-  uint64_t *udst[] = {id, parentId};
-  for (int k = 0; k < 2; ++k) {
-    if (!udst[k]) continue;
-    k_unpermute_u64<<<g, 256, 0, c->st>>>(usrc[k], c->cur.tag, (int)c->n, c->alt.id);
-    CK(cudaMemcpyAsync(udst[k], c->alt.id, c->n * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-  }
+  // radius, id and parent are slot-indexed already
+  if (radius) CK(cudaMemcpyAsync(radius, c->cur.radius, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (id) CK(cudaMemcpyAsync(id, c->cur.id, c->n * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->st));
+  if (parentId)
+    CK(cudaMemcpyAsync(parentId, c->cur.parent, c->n * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
   if (activity) {
     k_unpermute_act<<<g, 256, 0, c->st>>>(c->cur.tag, (int)c->n, (int8_t *)c->alt.tag);
     CK(cudaMemcpyAsync(activity, c->alt.tag, c->n, cudaMemcpyDeviceToHost, c->st));
@@ -1215,27 +1232,33 @@ int ladds_gpu_integrate(ladds_gpu_ctx *c, int steps) {
 namespace {
 // Compaction of the objects flagged keep[j] = 1 in scratchA (current order;
 // scratchC holds the same flags in slot order): survivors keep their
-// relative slot order and are renumbered 0..n'-1; the pre-compaction state
-// is left in c->alt.  hKeep (may be NULL) receives the flags.
-int compactKept(ladds_gpu_ctx *c, std::vector<uint32_t> *hKeep) {
+// relative slot order and are renumbered 0..n'-1.  The slot-indexed arrays
+// are compacted through the roll-back buffer's positions and velocities,
+// which hold nothing between calls.
+int compactKept(ladds_gpu_ctx *c) {
   const int n = (int)c->n;
   uint32_t *keep = c->scratchA, *pos = c->scratchB, *aliveBySlot = c->scratchC, *newSlot = c->keys1;
   // exclusive scans: positions in the current order, new slot numbers in slot order
   enqueueExclusiveScan(c, keep, (size_t)n, pos);
   enqueueExclusiveScan(c, aliveBySlot, (size_t)n, newSlot);
   CK(cudaGetLastError());
-  k_compact<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, c->alt, keep, pos, newSlot, n);
+  double *tRadius = c->snap.x;
+  auto *tId = reinterpret_cast<uint64_t *>(c->snap.y), *tParent = reinterpret_cast<uint64_t *>(c->snap.z);
+  k_compact<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, c->alt, keep, pos, newSlot, n, tRadius, tId, tParent);
   uint32_t kept = 0, lastKeep = 0;
   CK(cudaMemcpyAsync(&kept, pos + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(&lastKeep, keep + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
-  if (hKeep) {
-    hKeep->resize(n);
-    CK(cudaMemcpyAsync(hKeep->data(), keep, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
-  }
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
+  const size_t m = (size_t)kept + lastKeep;
+  if (m) {  // back into the shared slot-indexed arrays
+    CK(cudaMemcpyAsync(c->cur.radius, tRadius, m * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->cur.id, tId, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->cur.parent, tParent, m * sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
   std::swap(c->cur, c->alt);
-  c->n = (size_t)kept + lastKeep;
+  c->n = m;
   c->orderValid = false;
   dropGraphs(c);
   return LADDS_OK;
@@ -1540,18 +1563,18 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
   if (!burnt) return LADDS_OK;  // nothing burns up: the state, its order and the captured graphs stay
-  std::vector<uint32_t> hKeep;
-  int rc = compactKept(c, &hKeep);
-  if (rc) return rc;
-  const size_t removed = (size_t)n - c->n;
-  if (removedIds && removed) {  // ids of the removed objects from the pre-compaction buffer
+  if (removedIds) {  // ids of the removed objects, in slot order, before the compaction renumbers them
+    std::vector<uint32_t> alive(n);
     std::vector<uint64_t> ids(n);
-    CK(cudaMemcpy(ids.data(), c->alt.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(alive.data(), c->scratchC, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ids.data(), c->cur.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
     size_t w = 0;
     for (int i = 0; i < n && w < cap; ++i)
-      if (!hKeep[i]) removedIds[w++] = ids[i];
+      if (!alive[i]) removedIds[w++] = ids[i];
   }
-  if (nRemoved) *nRemoved = removed;
+  int rc = compactKept(c);
+  if (rc) return rc;
+  if (nRemoved) *nRemoved = (size_t)n - c->n;
   return LADDS_OK;
 }
 
@@ -1568,7 +1591,7 @@ int ladds_gpu_remove_slots(ladds_gpu_ctx *c, const uint32_t *slots, size_t m) {
   CK(cudaMemcpyAsync(dMark, mark.data(), c->n, cudaMemcpyHostToDevice, c->st));
   k_slot_mark_flags<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.tag, (int)c->n, dMark, c->scratchA,
                                                               c->scratchC);
-  return compactKept(c, nullptr);
+  return compactKept(c);
 }
 
 int ladds_gpu_select_layers(ladds_gpu_ctx *c, int32_t izLo, int32_t izHi, uint32_t *slots, size_t cap, size_t *n) {

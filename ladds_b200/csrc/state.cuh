@@ -25,6 +25,10 @@ __host__ __device__ __forceinline__ uint32_t tagSlot(uint32_t t) { return t & kT
 __host__ __device__ __forceinline__ int tagAct(uint32_t t) { return (int)((t >> kTagActShift) & 3u); }
 __host__ __device__ __forceinline__ bool tagDummy(uint32_t t) { return (t & kTagDummy) != 0; }
 
+// One state buffer.  x .. vz, aom, bc and tag are indexed by position (the
+// order the buffer holds the objects in); radius, id and parent are indexed by
+// slot (tagSlot of the tag), do not move when the population is gathered into
+// cell order, and are shared by a context's buffers.
 struct DevState {
   double *x, *y, *z, *vx, *vy, *vz;
   double *aom, *bc, *radius;
