@@ -385,7 +385,10 @@ class Context:
 
     def remove_below(self, min_altitude: float):
         n = self.size()
-        ids = np.zeros(max(n, 1), dtype=np.uint64)
+        # one id buffer reused across calls (a fresh population-sized buffer per call costs more than the call)
+        if getattr(self, "_removed_ids", None) is None or len(self._removed_ids) < max(n, 1):
+            self._removed_ids = np.empty(max(n, 1), dtype=np.uint64)
+        ids = self._removed_ids
         removed = C.c_size_t()
         self._check(self._L.ladds_gpu_remove_below(self._h, min_altitude, C.byref(removed), _p(ids), n))
         return ids[: removed.value].copy()

@@ -35,6 +35,7 @@ class HotPathLoop {
   GpuContext &gpu_;
   double deltaT_, minAltitude_, cutoff_, factor_, minDetectionRadius_, evasionCutoff_, conjunctionThreshold_;
   size_t k_;
+  std::vector<uint64_t> removedIds_;  // ids of the iteration's burn-ups (kept between iterations)
   size_t iteration_ = 0, iterationsSinceLastCollision_ = 0, totalEvasions_ = 0;
   Writer writeCollisions_, writeEvasions_;
 };

@@ -436,16 +436,16 @@ size_t HotPathLoop::run(size_t n) {
     gpu_.check(ladds_gpu_integrate(gpu_.handle(), 1));
     // burn-ups: removed on the device and, by id, from the container
     const size_t before = gpu_.deviceSize();
-    std::vector<uint64_t> removed(before);
+    if (removedIds_.size() < before) removedIds_.resize(before);  // reused: no population-sized buffer per iteration
+    std::vector<uint64_t> &removed = removedIds_;
     size_t nRemoved = 0;
-    gpu_.check(ladds_gpu_remove_below(gpu_.handle(), minAltitude_, &nRemoved, removed.data(), removed.size()));
+    gpu_.check(ladds_gpu_remove_below(gpu_.handle(), minAltitude_, &nRemoved, removed.data(), before));
     if (nRemoved) {
-      removed.resize(nRemoved);
-      std::sort(removed.begin(), removed.end());
+      std::vector<uint64_t> gone(removed.begin(), removed.begin() + (std::ptrdiff_t)std::min(nRemoved, before));
+      std::sort(gone.begin(), gone.end());
       container_.erase(std::remove_if(container_.begin(), container_.end(),
                                       [&](const Particle &p) {
-                                        return std::binary_search(removed.begin(), removed.end(),
-                                                                  (uint64_t)p.getID());
+                                        return std::binary_search(gone.begin(), gone.end(), (uint64_t)p.getID());
                                       }),
                        container_.end());
       gpu_.markMirrored(container_);
