@@ -72,6 +72,7 @@ struct ladds_gpu_ctx {
   cudaStream_t st = nullptr;   // main stream
   cudaStream_t st2 = nullptr;  // pair scans, overlapped with the next propagation
   cudaEvent_t evCells = nullptr, evScan = nullptr;
+  cudaEvent_t evXfer[7] = {};  // per-array hand-offs between copies and (un)permutes of set/get_state
   int64_t *dIterBase = nullptr;  // first iteration of the chunk being run (device)
   size_t n = 0, cap = 0;
   DevState cur{}, alt{}, snap{};
@@ -339,9 +340,9 @@ int ensureCandCapacity(ladds_gpu_ctx *c, size_t need) {
 // After a scan call: grows the record / candidate buffers that overflowed.
 // *overflow tells whether the call has to be re-run.
 int growIfOverflowed(ladds_gpu_ctx *c, unsigned long long *records, bool *overflow) {
-  unsigned long long cnt = 0, need = 0;
-  CK(cudaMemcpy(&cnt, c->dCount, sizeof(cnt), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(&need, c->dCandNeed, sizeof(need), cudaMemcpyDeviceToHost));
+  unsigned long long words[2] = {0, 0};  // record count, largest candidate count (adjacent)
+  CK(cudaMemcpy(words, c->dCount, sizeof(words), cudaMemcpyDeviceToHost));
+  const unsigned long long cnt = words[0], need = words[1];
   *records = cnt;
   *overflow = cnt > c->pairCap || need > c->candCap;
   if (cnt > c->pairCap) {
@@ -888,12 +889,12 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   c->dCandNeed = c->dCount + 1;
   c->dStatus = reinterpret_cast<unsigned *>(c->dCount + 2);
   cudaMemset(c->dCount, 0, 3 * sizeof(unsigned long long));
-  cudaMemset(c->dCount, 0, sizeof(unsigned long long));
   cudaMemset(c->dIter, 0, 2 * sizeof(int64_t));
   cudaEventCreate(&c->callStart);
   cudaEventCreate(&c->callEnd);
   cudaEventCreateWithFlags(&c->evCells, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
+  for (auto &e : c->evXfer) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   cudaMemset(c->dCandCount, 0, 2 * sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
@@ -935,6 +936,8 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   if (c->callEnd) cudaEventDestroy(c->callEnd);
   if (c->evCells) cudaEventDestroy(c->evCells);
   if (c->evScan) cudaEventDestroy(c->evScan);
+  for (auto e : c->evXfer)
+    if (e) cudaEventDestroy(e);
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -1143,11 +1146,15 @@ int ladds_gpu_set_state(ladds_gpu_ctx *c, size_t n, const double *x, const doubl
   double *dst[] = {c->cur.x, c->cur.y, c->cur.z, c->cur.vx, c->cur.vy, c->cur.vz};
   double *stage[] = {c->alt.x, c->alt.y, c->alt.z, c->alt.vx, c->alt.vy, c->alt.vz};
   const int g = blocksFor(n, 256);
+  // the copies run back to back on the main stream; each array's gather into
+  // cell order runs on the second stream while the next array crosses PCIe
   for (int k = 0; k < 6; ++k) {
     CK(cudaMemcpyAsync(stage[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    k_permute_from_slots_f64<<<g, 256, 0, c->st>>>(stage[k], c->cur.tag, (int)n, dst[k]);
+    CK(cudaEventRecord(c->evXfer[k], c->st));
+    CK(cudaStreamWaitEvent(c->st2, c->evXfer[k], 0));
+    k_permute_from_slots_f64<<<g, 256, 0, c->st2>>>(stage[k], c->cur.tag, (int)n, dst[k]);
   }
-  CK(cudaStreamSynchronize(c->st));
+  CK(cudaStreamSynchronize(c->st2));
   CK(cudaGetLastError());
   return LADDS_OK;
 }
@@ -1163,9 +1170,19 @@ int ladds_gpu_get_state(ladds_gpu_ctx *c, size_t n, double *x, double *y, double
   double *stage[] = {c->alt.x, c->alt.y, c->alt.z, c->alt.vx, c->alt.vy, c->alt.vz};
   double *dst[] = {x, y, z, vx, vy, vz};
   const int g = blocksFor(c->n, 256);
+  // scatters into slot order on the second stream, all launched before the
+  // first copy (a copy into pageable memory blocks the host); each array's
+  // copy waits for its own scatter only
+  CK(cudaEventRecord(c->evXfer[6], c->st));
+  CK(cudaStreamWaitEvent(c->st2, c->evXfer[6], 0));
   for (int k = 0; k < 6; ++k) {
     if (!dst[k]) continue;
-    k_unpermute_f64<<<g, 256, 0, c->st>>>(src[k], c->cur.tag, (int)c->n, stage[k]);
+    k_unpermute_f64<<<g, 256, 0, c->st2>>>(src[k], c->cur.tag, (int)c->n, stage[k]);
+    CK(cudaEventRecord(c->evXfer[k], c->st2));
+  }
+  for (int k = 0; k < 6; ++k) {
+    if (!dst[k]) continue;
+    CK(cudaStreamWaitEvent(c->st, c->evXfer[k], 0));
     CK(cudaMemcpyAsync(dst[k], stage[k], c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   }
   CK(cudaStreamSynchronize(c->st));

@@ -446,3 +446,35 @@ def test_threshold_neighbourhood_records_bitexact(capi, oracle, near_rel):
     if near_rel >= 1e-6:
         near = capi.PAIR_NEAR_COLLISION | capi.PAIR_NEAR_EVASION | capi.PAIR_NEAR_CONJUNCTION | capi.PAIR_NEAR_GATE
         assert np.sum((ref["flags"] & near) != 0) > 50
+
+
+# ---------------------------------------------------------------- host-owned state
+def test_host_owned_state_round_trip(capi, oracle):
+    """set_state / get_state exchange positions and velocities in slot (upload)
+    order while the device keeps the population in cell order: get_state equals
+    download, a set_state'd state comes back unchanged, and the records of a
+    scan after set_state are the oracle's for that state."""
+    pop = dense_population(21, n=4000)
+    rng = np.random.default_rng(5)
+    with ctx_for(capi, deltaT=1.0, componentMask=capi.KEP | capi.J2, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        ctx.step(3)  # the device order is now the cell order, not the upload order
+        _, slots = ctx.cell_order()
+        assert not np.array_equal(slots, np.arange(len(slots)))
+        got = ctx.get_state()
+        down = ctx.download()
+        for a, k in zip(got, ("x", "y", "z", "vx", "vy", "vz")):
+            assert np.array_equal(a, down[k])
+        new = [a + rng.normal(scale=0.5 if i < 3 else 1e-3, size=a.shape) for i, a in enumerate(got)]
+        ctx.set_state(*new)
+        for a, b in zip(ctx.get_state(), new):
+            assert np.array_equal(a, b)
+        recs = ctx.conjunctions(1.0)
+        state = ctx.download()
+    for k, a in zip(("x", "y", "z", "vx", "vy", "vz"), new):
+        assert np.array_equal(state[k], a)
+    p = oracle.scan_params(cutoff=20.0, dt=1.0, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    ref = oracle.scan_bruteforce(to_oracle(oracle, state), p, step=2)  # records carry the last iteration
+    assert len(ref) > 20
+    assert records_equal(recs, ref), describe_diff(recs, ref)
