@@ -391,10 +391,11 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    world, rank, local = dist_init(args)
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        # rank 0 alone times the CPU path; no process group (there is no collective)
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_init(args)
 
     from ladds_b200 import build, capi
 
