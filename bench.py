@@ -11,9 +11,9 @@ Yoshida-4 step of every object, then the conjunction scan.  ``value`` is the
 split-precision object-steps/s with the population resident in HBM; the FP64
 figure, their ratio and the one-day RMS drift of split vs FP64 are reported
 beside it.  ``e2e`` runs the same steps through the C ABI in the host-owned
-mode of the drop-in: per step the positions/velocities go host->device from
-pinned memory, the step runs, positions/velocities and the conjunction
-records come back; ``e2e.device_resident`` is the drop-in's own data flow, the
+mode of the drop-in (ladds_gpu_step_host): per step the positions/velocities
+go host->device from pinned memory, the step runs, positions/velocities and
+the conjunction records come back; ``e2e.device_resident`` is the drop-in's own data flow, the
 population kept on the device and each iteration's records read back.
 ``--impl reference`` times the CPU restatement of the reference path (the
 oracle; the reference itself cannot be built here).
@@ -481,19 +481,30 @@ def main():
         for a, b in zip(pinned, st):
             a[:] = b
         out = np.zeros(1 << 16, dtype=capi.PAIR_DTYPE)
+        ctx.step_host(pinned, out=out)  # warm-up
         dist_barrier(world)
         t0 = time.perf_counter()
         rec_bytes = 0
         for _ in range(args.e2e_steps):
-            ctx.set_state(*pinned)
-            r = ctx.step(1, out=out)
+            r = ctx.step_host(pinned, out=out)
             rec_bytes += len(r.records) * 64 + 8
-            ctx._check(ctx._L.ladds_gpu_get_state(ctx.handle, n, *[a.ctypes.data_as(capi.C.c_void_p)
-                                                                    for a in pinned]))
         el = dist_max(time.perf_counter() - t0, world)
         e2e = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": int(48 * n + rec_bytes / args.e2e_steps),
-               "steps": args.e2e_steps, "mode": "host-owned state (set_state / step(1) / get_state, pinned)"}
+               "steps": args.e2e_steps,
+               "mode": "host-owned state, pinned: ladds_gpu_step_host per iteration (chunked copies in and out "
+                       "overlapped with the propagation and the scan)"}
+        # the same iterations as three calls: set_state / step(1) / get_state
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ctx.set_state(*pinned)
+            ctx.step(1, out=out)
+            ctx._check(ctx._L.ladds_gpu_get_state(ctx.handle, n, *[a.ctypes.data_as(capi.C.c_void_p)
+                                                                    for a in pinned]))
+        el = dist_max(time.perf_counter() - t0, world)
+        e2e["three_calls"] = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
+                              "mode": "set_state / step(1) / get_state per iteration, pinned"}
         # the drop-in's own data flow (ladds::HotPathLoop): the population stays on the device and
         # each iteration's records come back to the host (pinned) from one ladds_gpu_step(1) call
         outp = torch.empty((1 << 16) * capi.PAIR_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True).numpy()

@@ -216,6 +216,26 @@ int ladds_gpu_scan(ladds_gpu_ctx *ctx, const ladds_scan_params *params, ladds_pa
 int ladds_gpu_step(ladds_gpu_ctx *ctx, int iterations, ladds_pair *out, size_t cap, size_t *nOut,
                    ladds_step_stats *stats);
 
+/* One iteration of the reference loop (Simulation.cpp:287-415) for a caller
+ * that keeps the population's positions and velocities in host memory between
+ * iterations, as the reference's AutoPas container does (Simulation.cpp:297
+ * integrates it in place): `in` holds x, y, z, vx, vy, vz of the n objects in
+ * upload (slot) order at the start of the iteration, `outState` receives them
+ * after the step (`outState` may be `in`: the update is then in place).  The
+ * arrays cross PCIe in up to 4 chunks: a chunk is propagated as soon as it is
+ * on the device and copied back while the next one comes in (both PCIe
+ * directions at once; pinned host memory is needed for the copies to overlap).
+ * The scan (when iteration % k == 0) follows the propagation.  The result equals ladds_gpu_set_state + ladds_gpu_step(1) +
+ * ladds_gpu_get_state, bit for bit.  LADDS_ERR_CAPACITY: the
+ * iteration HAS been taken (outState holds its state), *nOut is the number of
+ * records and ladds_gpu_pending_records returns them.  Other errors: the
+ * iteration is not counted and outState is unspecified. */
+int ladds_gpu_step_host(ladds_gpu_ctx *ctx, size_t n, const double *const in[6], double *const outState[6],
+                        ladds_pair *out, size_t cap, size_t *nOut, ladds_step_stats *stats);
+/* The records held back by the last ladds_gpu_step_host that returned
+ * LADDS_ERR_CAPACITY (capacity handling as above; they are released once read). */
+int ladds_gpu_pending_records(ladds_gpu_ctx *ctx, ladds_pair *out, size_t cap, size_t *nOut);
+
 /* Deletes particles with |r| < R_EARTH + minAltitude (Simulation.cpp:561-596);
  * survivors keep their relative slot order and are renumbered 0..n'-1.
  * removedIds (may be NULL) receives up to cap ids of removed particles. */

@@ -88,7 +88,7 @@ EXPORTED = [
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
     "ladds_records_write_csv", "ladds_gpu_checked_insert", "ladds_gpu_get_objects", "ladds_breakup_collision",
     "ladds_gpu_breakup", "ladds_gpu_select_layers", "ladds_gpu_layer_histogram", "ladds_gpu_remove_slots",
-    "ladds_gpu_set_halo",
+    "ladds_gpu_set_halo", "ladds_gpu_step_host", "ladds_gpu_pending_records",
 ]
 
 STATE_RECORD_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("aom", "<f8"),
@@ -156,6 +156,9 @@ def lib():
     L.ladds_gpu_conjunctions.argtypes = [vp, C.c_double, vp, sz, C.POINTER(sz), C.POINTER(sz), C.POINTER(sz),
                                          C.POINTER(sz)]
     L.ladds_gpu_step.argtypes = [vp, i, vp, sz, C.POINTER(sz), C.POINTER(StepStats)]
+    L.ladds_gpu_step_host.argtypes = [vp, sz, C.POINTER(vp), C.POINTER(vp), vp, sz, C.POINTER(sz),
+                                      C.POINTER(StepStats)]
+    L.ladds_gpu_pending_records.argtypes = [vp, vp, sz, C.POINTER(sz)]
     L.ladds_gpu_remove_below.argtypes = [vp, C.c_double, C.POINTER(sz), vp, sz]
     L.ladds_gpu_mark_deleted.argtypes = [vp, vp, sz]
     L.ladds_gpu_clear_parents.argtypes = [vp]
@@ -367,6 +370,33 @@ class Context:
                 continue
             self._check(rc)
             return StepResult(buf[: n.value].copy(), st)
+
+    def step_host(self, state_in, state_out=None, out: np.ndarray | None = None) -> StepResult:
+        """One iteration with the positions and velocities in host memory
+        (ladds_gpu_step_host): state_in = (x, y, z, vx, vy, vz) float64 arrays in
+        slot order; state_out receives the new state (default: state_in, in place).
+        Pinned arrays (torch pin_memory) let the copies overlap."""
+        n = self.size()
+        ins = list(state_in)
+        outs = ins if state_out is None else list(state_out)
+        if len(ins) != 6 or len(outs) != 6:
+            raise ValueError("six state arrays: x, y, z, vx, vy, vz")
+        for a in ins + outs:
+            if a.shape != (n,) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("state arrays must be contiguous float64 of the population size")
+        if any(not a.flags.writeable for a in outs):
+            raise ValueError("state_out arrays must be writeable")
+        buf = out if out is not None else np.zeros(4096, dtype=PAIR_DTYPE)
+        got = C.c_size_t()
+        st = StepStats()
+        rc = self._L.ladds_gpu_step_host(self._h, n, (C.c_void_p * 6)(*[a.ctypes.data for a in ins]),
+                                         (C.c_void_p * 6)(*[a.ctypes.data for a in outs]), _p(buf), len(buf),
+                                         C.byref(got), C.byref(st))
+        if rc == ERR_CAPACITY and got.value > len(buf):  # the iteration was taken; its records wait
+            buf = np.zeros(got.value, dtype=PAIR_DTYPE)
+            rc = self._L.ladds_gpu_pending_records(self._h, _p(buf), len(buf), C.byref(got))
+        self._check(rc)
+        return StepResult(buf[: got.value].copy(), st)
 
     def cell_order(self):
         n = self.size()

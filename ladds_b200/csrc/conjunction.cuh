@@ -238,6 +238,10 @@ __global__ void k_unpermute_act(const uint32_t *__restrict__ tag, int n, int8_t 
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = (int8_t)tagAct(tag[j]);
 }
+__global__ void k_unpermute_tag(const uint32_t *__restrict__ tag, int n, uint32_t *__restrict__ dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && tagSlot(tag[j]) < (uint32_t)n) dst[tagSlot(tag[j])] = tag[j];
+}
 // Gather slot-ordered values into the current (sorted) order (state upload).
 __global__ void k_permute_from_slots_f64(const double *__restrict__ src, const uint32_t *__restrict__ tag, int n,
                                          double *__restrict__ dst) {

@@ -60,6 +60,11 @@ inline int blocksFor(size_t n, int b) { return (int)((n + (size_t)b - 1) / (size
 
 enum Phase { kPhProp, kPhBucket, kPhRowsort, kPhPermute, kPhCandidates, kPhEvaluate };
 
+// ladds_gpu_step_host moves the state in at most this many chunks, each at
+// least kHostChunkMin objects (smaller copies cost more than they overlap)
+constexpr int kHostChunks = 4;
+constexpr size_t kHostChunkMin = (size_t)1 << 17;
+
 }  // namespace
 
 struct ladds_gpu_ctx {
@@ -71,8 +76,11 @@ struct ladds_gpu_ctx {
   int dev = 0;
   cudaStream_t st = nullptr;   // main stream
   cudaStream_t st2 = nullptr;  // pair scans, overlapped with the next propagation
+  cudaStream_t st3 = nullptr;  // device-to-host copies of ladds_gpu_step_host
   cudaEvent_t evCells = nullptr, evScan = nullptr;
   cudaEvent_t evXfer[7] = {};  // per-array hand-offs between copies and (un)permutes of set/get_state
+  cudaEvent_t evPipe[2 * kHostChunks + 1] = {};  // chunk hand-offs of ladds_gpu_step_host
+  std::vector<ladds_pair> pending;  // records of a ladds_gpu_step_host call whose buffer was too small
   int64_t *dIterBase = nullptr;  // first iteration of the chunk being run (device)
   size_t n = 0, cap = 0;
   DevState cur{}, alt{}, snap{};
@@ -439,6 +447,30 @@ cudaError_t enqueueEphemeris(ladds_gpu_ctx *c, int nSteps) {
                                  c->st);
 }
 
+// the propagation kernel over objects [0, n) of s on the main stream; with
+// keys, their cell keys and row arrivals go to keyOut / arrOut (indexed as s)
+void launchPropagate(ladds_gpu_ctx *c, const DevState &s, int n, int nSteps, int ephBase, bool keys,
+                     uint32_t *keyOut, uint32_t *arrOut) {
+  const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
+  const int g = blocksFor((size_t)n, b);
+  uint32_t *rc = c->rowCounts;
+  if (c->cfg.precision == LADDS_PRECISION_SPLIT) {
+    if (keys)
+      k_propagate<true, true><<<g, b, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc, arrOut,
+                                                  c->dStatus);
+    else
+      k_propagate<true, false><<<g, b, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr, nullptr,
+                                                   c->dStatus);
+  } else {
+    if (keys)
+      k_propagate<false, true><<<g, b, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc, arrOut,
+                                                   c->dStatus);
+    else
+      k_propagate<false, false><<<g, b, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr,
+                                                    nullptr, c->dStatus);
+  }
+}
+
 // nSteps steps whose stage ephemerides are c_eph[ephBase ...]
 void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
   if (c->n == 0) {
@@ -448,26 +480,7 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
   // with keys: the row counts of the coming sort are accumulated by the kernel
   if (keys) cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st);
   PhaseScope ps(c, kPhProp, c->st, 2);  // propagation + iteration counter
-  const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
-  const int g = blocksFor(c->n, b);
-  const int n = (int)c->n;
-  const bool split = c->cfg.precision == LADDS_PRECISION_SPLIT;
-  uint32_t *rc = c->rowCounts, *arr = c->scratchC;
-  if (split) {
-    if (keys)
-      k_propagate<true, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, rc, arr,
-                                                  c->dStatus);
-    else
-      k_propagate<true, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr,
-                                                   nullptr, c->dStatus);
-  } else {
-    if (keys)
-      k_propagate<false, true><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, c->keys0, rc, arr,
-                                                   c->dStatus);
-    else
-      k_propagate<false, false><<<g, b, 0, c->st>>>(c->cur, n, nSteps, ephBase, c->pc, c->grid, nullptr, nullptr,
-                                                    nullptr, c->dStatus);
-  }
+  launchPropagate(c, c->cur, (int)c->n, nSteps, ephBase, keys, c->keys0, c->scratchC);
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, nSteps);
 }
 
@@ -879,7 +892,8 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       cudaMalloc(&c->dCandCount, 2 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
       cudaMalloc(&c->dIter, 2 * sizeof(int64_t)) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     ladds_gpu_destroy(c);
     return LADDS_ERR_ALLOC;
@@ -895,6 +909,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaEventCreateWithFlags(&c->evCells, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
   for (auto &e : c->evXfer) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  for (auto &e : c->evPipe) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   cudaMemset(c->dCandCount, 0, 2 * sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
@@ -938,6 +953,9 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   if (c->evScan) cudaEventDestroy(c->evScan);
   for (auto e : c->evXfer)
     if (e) cudaEventDestroy(e);
+  for (auto e : c->evPipe)
+    if (e) cudaEventDestroy(e);
+  if (c->st3) cudaStreamDestroy(c->st3);
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -1504,6 +1522,152 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
       stats->conjunctions += (p.flags & LADDS_PAIR_CONJUNCTION) != 0;
     }
   }
+  return LADDS_OK;
+}
+
+int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], double *const outState[6],
+                        ladds_pair *out, size_t cap, size_t *nOut, ladds_step_stats *stats) {
+  if (!c || !in || !outState || !nOut) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  *nOut = 0;
+  if (n != c->n) return fail(c, LADDS_ERR_INVALID_ARG, "step_host: n differs from the population size");
+  for (int a = 0; a < 6; ++a)
+    if (n && (!in[a] || !outState[a])) return fail(c, LADDS_ERR_INVALID_ARG, "null array pointer");
+  CK(cudaSetDevice(c->dev));
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  c->pending.clear();
+  const int k = c->cfg.timestepsPerCollisionDetection;
+  const bool scan = (c->hostIter % k) == 0 && n;
+  const int64_t startIter = c->hostIter;
+  // the iteration's source buffer, in slot order: positions and velocities
+  // from the host, the per-object constants and tags scattered out of the
+  // current (cell-ordered) buffer
+  const DevState S = c->snap;
+  const int ni = (int)n;
+  CK(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
+  CK(cudaEventRecord(c->callStart, c->st));
+  if (n) {
+    const int g = blocksFor(n, 256);
+    k_unpermute_f64<<<g, 256, 0, c->st>>>(c->cur.aom, c->cur.tag, ni, S.aom);
+    k_unpermute_f64<<<g, 256, 0, c->st>>>(c->cur.bc, c->cur.tag, ni, S.bc);
+    k_unpermute_tag<<<g, 256, 0, c->st>>>(c->cur.tag, ni, S.tag);
+  }
+  CK(enqueueEphemeris(c, 1));
+  if (scan) CK(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
+  // chunks: host->device on st2, propagation on st, device->host on st3
+  const int chunks = (int)std::max<size_t>(1, std::min<size_t>((size_t)kHostChunks, n / kHostChunkMin));
+  const size_t per = (n + (size_t)chunks - 1) / (size_t)chunks;
+  double *const sArr[6] = {S.x, S.y, S.z, S.vx, S.vy, S.vz};
+  int used = 0;
+  for (int ch = 0; ch < chunks && n; ++ch) {
+    const size_t lo = (size_t)ch * per;
+    if (lo >= n) break;
+    const size_t len = std::min(per, n - lo);
+    for (int a = 0; a < 6; ++a)
+      CK(cudaMemcpyAsync(sArr[a] + lo, in[a] + lo, len * sizeof(double), cudaMemcpyHostToDevice, c->st2));
+    CK(cudaEventRecord(c->evPipe[2 * ch], c->st2));
+    CK(cudaStreamWaitEvent(c->st, c->evPipe[2 * ch], 0));
+    DevState Sc = S;
+    Sc.x += lo; Sc.y += lo; Sc.z += lo; Sc.vx += lo; Sc.vy += lo; Sc.vz += lo;
+    Sc.aom += lo; Sc.bc += lo; Sc.tag += lo;
+    launchPropagate(c, Sc, (int)len, 1, 0, scan, c->keys0 + lo, c->scratchC + lo);
+    CK(cudaEventRecord(c->evPipe[2 * ch + 1], c->st));
+    CK(cudaStreamWaitEvent(c->st3, c->evPipe[2 * ch + 1], 0));
+    for (int a = 0; a < 6; ++a)
+      CK(cudaMemcpyAsync(outState[a] + lo, sArr[a] + lo, len * sizeof(double), cudaMemcpyDeviceToHost, c->st3));
+    used = ch + 1;
+  }
+  k_advance<<<1, 32, 0, c->st>>>(c->dIter, 1);
+  const DevState curStart = c->cur, altStart = c->alt;
+  ScanConsts sc = c->sc;
+  sc.dt = c->cfg.deltaT * (double)k;
+  if (scan) {
+    // sort and gather from the slot-ordered buffer into the other buffer of the
+    // pair, which becomes the current one (as after a scan of ladds_gpu_step)
+    c->cur = S;
+    c->alt = curStart;
+    enqueueSort(c);
+    c->alt = altStart;
+    enqueueCells(c);  // gathers S into altStart, then cur = altStart, alt = S (the scan reads alt)
+    enqueueScanWith(c, c->st, sc, c->cutF, c->dIterBase, 0);
+  } else if (n) {
+    // no scan: the new positions and velocities into the current buffer's order
+    const int g = blocksFor(n, 256);
+    double *const dst[6] = {c->cur.x, c->cur.y, c->cur.z, c->cur.vx, c->cur.vy, c->cur.vz};
+    for (int a = 0; a < 6; ++a) k_permute_from_slots_f64<<<g, 256, 0, c->st>>>(sArr[a], c->cur.tag, ni, dst[a]);
+  }
+  if (used) {
+    CK(cudaEventRecord(c->evPipe[2 * kHostChunks], c->st3));
+    CK(cudaStreamWaitEvent(c->st, c->evPipe[2 * kHostChunks], 0));
+  }
+  CK(cudaEventRecord(c->callEnd, c->st));
+  // the buffer roles after the call: S is the roll-back buffer again, the pair
+  // (cur, alt) is the one the captured graphs were made with
+  auto restoreRoles = [&]() {
+    if (scan) c->alt = curStart;
+  };
+  auto undo = [&](int rc) {
+    // the iteration is not counted; the device copy of the state is replaced by
+    // the next call's host state
+    restoreRoles();
+    cudaStreamSynchronize(c->st3);
+    cudaMemcpyAsync(c->dIter, &startIter, sizeof(int64_t), cudaMemcpyHostToDevice, c->st);
+    cudaStreamSynchronize(c->st);
+    c->orderValid = false;
+    return rc;
+  };
+  unsigned long long cnt = 0;
+  bool overflow = false;
+  int rc = syncStatusAndGrow(c, &cnt, &overflow);
+  collectTimes(c);
+  if (rc) return undo(rc);
+  int retries = 0;
+  while (overflow) {  // the device buffers have grown: the scan alone runs again on the same state
+    if (++retries > 4) return undo(fail(c, LADDS_ERR_CAPACITY, "device scan buffers kept overflowing"));
+    CK(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
+    enqueueScanWith(c, c->st, sc, c->cutF, c->dIterBase, 0);
+    rc = syncStatusAndGrow(c, &cnt, &overflow);
+    collectTimes(c);
+    if (rc) return undo(rc);
+  }
+  restoreRoles();
+  CK(cudaStreamSynchronize(c->st3));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->callStart, c->callEnd);
+  std::vector<ladds_pair> recs(cnt);
+  if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
+  std::sort(recs.begin(), recs.end(), pairLess);
+  c->hostIter += 1;
+  if (scan) c->orderValid = true;
+  if (stats) {
+    stats->iterations = 1;
+    stats->scans = scan ? 1 : 0;
+    stats->records = cnt;
+    stats->retries = (uint64_t)retries;
+    stats->deviceMs = ms;
+    for (const auto &p : recs) {
+      stats->collisions += (p.flags & LADDS_PAIR_COLLISION) != 0;
+      stats->evasions += (p.flags & LADDS_PAIR_EVASION) != 0;
+      stats->conjunctions += (p.flags & LADDS_PAIR_CONJUNCTION) != 0;
+    }
+  }
+  *nOut = recs.size();
+  if (recs.size() > cap || (!out && !recs.empty())) {
+    c->pending = std::move(recs);
+    return fail(c, LADDS_ERR_CAPACITY, "output buffer too small: the records wait in ladds_gpu_pending_records");
+  }
+  if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
+  return LADDS_OK;
+}
+
+int ladds_gpu_pending_records(ladds_gpu_ctx *c, ladds_pair *out, size_t cap, size_t *nOut) {
+  if (!c || !nOut) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  *nOut = c->pending.size();
+  if (c->pending.size() > cap || (!out && !c->pending.empty()))
+    return fail(c, LADDS_ERR_CAPACITY, "output buffer too small for the pending records");
+  if (!c->pending.empty()) std::memcpy(out, c->pending.data(), c->pending.size() * sizeof(ladds_pair));
+  c->pending.clear();
   return LADDS_OK;
 }
 
