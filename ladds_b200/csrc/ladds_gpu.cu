@@ -1579,6 +1579,17 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, 1);
   const DevState curStart = c->cur, altStart = c->alt;
+  // the buffer roles when the call returns (on every path): S is the roll-back
+  // buffer again and (cur, alt) the pair the captured graphs were made with;
+  // the scan reads S as alt until then
+  struct RoleGuard {
+    ladds_gpu_ctx *c;
+    DevState alt;
+    bool on;
+    ~RoleGuard() {
+      if (on) c->alt = alt;
+    }
+  } roles{c, curStart, scan};
   ScanConsts sc = c->sc;
   sc.dt = c->cfg.deltaT * (double)k;
   if (scan) {
@@ -1601,15 +1612,9 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     CK(cudaStreamWaitEvent(c->st, c->evPipe[2 * kHostChunks], 0));
   }
   CK(cudaEventRecord(c->callEnd, c->st));
-  // the buffer roles after the call: S is the roll-back buffer again, the pair
-  // (cur, alt) is the one the captured graphs were made with
-  auto restoreRoles = [&]() {
-    if (scan) c->alt = curStart;
-  };
   auto undo = [&](int rc) {
     // the iteration is not counted; the device copy of the state is replaced by
     // the next call's host state
-    restoreRoles();
     cudaStreamSynchronize(c->st3);
     cudaMemcpyAsync(c->dIter, &startIter, sizeof(int64_t), cudaMemcpyHostToDevice, c->st);
     cudaStreamSynchronize(c->st);
@@ -1623,14 +1628,13 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   if (rc) return undo(rc);
   int retries = 0;
   while (overflow) {  // the device buffers have grown: the scan alone runs again on the same state
-    if (++retries > 4) return undo(fail(c, LADDS_ERR_CAPACITY, "device scan buffers kept overflowing"));
+    if (++retries > 4) return undo(fail(c, LADDS_ERR_STATE, "device scan buffers kept overflowing"));
     CK(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
     enqueueScanWith(c, c->st, sc, c->cutF, c->dIterBase, 0);
     rc = syncStatusAndGrow(c, &cnt, &overflow);
     collectTimes(c);
     if (rc) return undo(rc);
   }
-  restoreRoles();
   CK(cudaStreamSynchronize(c->st3));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->callStart, c->callEnd);
