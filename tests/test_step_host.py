@@ -33,12 +33,15 @@ def pinned_state(arrays):
     return out
 
 
-def run_pair(capi, pop, iters, precision, k=1, pair_cap=1 << 16, in_place=True, pinned=True):
+def run_pair(capi, pop, iters, precision, k=1, pair_cap=1 << 16, in_place=True, pinned=True, pre=0):
     kw = dict(componentMask=capi.PROP_ALL, precision=precision, conjunctionThreshold=10.0,
               timestepsPerCollisionDetection=k, pairCapacity=pair_cap)
     with capi.Context(capi.default_config(**kw)) as a, capi.Context(capi.default_config(**kw)) as b:
         a.upload(pop)
         b.upload(pop)
+        if pre:  # graph-replayed iterations first: step_host must keep the buffer roles they were made with
+            assert records_equal(a.step(pre).records, b.step(pre).records)
+            pop = dict(zip(("x", "y", "z", "vx", "vy", "vz"), a.get_state()))
         # pinned: asynchronous copies that overlap; pageable: staged by the driver
         stage = pinned_state if pinned else (lambda arrays: [np.array(a, dtype=np.float64) for a in arrays])
         host = stage([pop[f] for f in ("x", "y", "z", "vx", "vy", "vz")])
@@ -58,7 +61,7 @@ def run_pair(capi, pop, iters, precision, k=1, pair_cap=1 << 16, in_place=True, 
             assert records_equal(ra.records, rb.records), describe_diff(ra.records, rb.records)
             assert int(rb.stats.records) == len(rb.records) and int(rb.stats.iterations) == 1
             total += len(rb.records)
-        assert a.iteration() == b.iteration() == iters
+        assert a.iteration() == b.iteration() == iters + pre
         da, db = a.download(), b.download()
         for f in da:
             assert np.array_equal(da[f], db[f]), f
@@ -90,6 +93,12 @@ def test_step_host_matches_three_calls_fp64_out_of_place(capi):
 def test_step_host_iterations_without_scan(capi):
     pop = capi.generate_population(0, 2026, 300_000)
     run_pair(capi, pop, 4, capi.PRECISION_SPLIT, k=3)
+
+
+@pytest.mark.parametrize("pre", [1, 2, 5])
+def test_step_host_after_graph_replayed_steps(capi, pre):
+    pop = capi.generate_population(0, 2031, 300_000)
+    run_pair(capi, pop, 3, capi.PRECISION_SPLIT, pre=pre)
 
 
 def test_step_host_device_buffer_growth(capi):
