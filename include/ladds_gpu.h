@@ -490,6 +490,20 @@ int ladds_gpu_adjoint_make_pairs(ladds_gpu_ctx *ctx, uint64_t seed, size_t nPair
 int ladds_population_generate(int which, uint64_t seed, size_t n, double *x, double *y, double *z, double *vx,
                               double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
                               uint64_t *parentId, int8_t *activity);
+/* Binary SoA population file, the input format shared by the library, the
+ * oracle and the benchmark (the reference reads CSV / HDF5 populations,
+ * io/DatasetReader.cpp, io/SatelliteLoader.cpp:17-128): a 24-byte
+ * little-endian header {"LADDSPOP", u32 version 1, u32 fields 12, u64 n}, then
+ * the twelve arrays of ladds_gpu_upload's order, n each.  read: *n = the file's
+ * count (LADDS_ERR_CAPACITY when above cap); NULL arrays are skipped; a file of
+ * another format or length is LADDS_ERR_INVALID_ARG. */
+int ladds_population_write(const char *path, size_t n, const double *x, const double *y, const double *z,
+                           const double *vx, const double *vy, const double *vz, const double *radius,
+                           const double *aom, const double *bcInv, const uint64_t *id, const uint64_t *parentId,
+                           const int8_t *activity);
+int ladds_population_read(const char *path, size_t cap, size_t *n, double *x, double *y, double *z, double *vx,
+                          double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
+                          uint64_t *parentId, int8_t *activity);
 /* Keplerian elements -> Cartesian state (km, km/s), Kepler's equation by Newton. */
 int ladds_elements_to_state(double a, double e, double inc, double raan, double argp, double meanAnomaly,
                             double r[3], double v[3]);

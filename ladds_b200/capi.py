@@ -88,7 +88,8 @@ EXPORTED = [
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
     "ladds_records_write_csv", "ladds_gpu_checked_insert", "ladds_gpu_get_objects", "ladds_breakup_collision",
     "ladds_gpu_breakup", "ladds_gpu_select_layers", "ladds_gpu_layer_histogram", "ladds_gpu_remove_slots",
-    "ladds_gpu_set_halo", "ladds_gpu_step_host", "ladds_gpu_pending_records",
+    "ladds_gpu_set_halo", "ladds_gpu_step_host", "ladds_gpu_pending_records", "ladds_population_write",
+    "ladds_population_read",
 ]
 
 STATE_RECORD_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("aom", "<f8"),
@@ -156,6 +157,8 @@ def lib():
     L.ladds_gpu_conjunctions.argtypes = [vp, C.c_double, vp, sz, C.POINTER(sz), C.POINTER(sz), C.POINTER(sz),
                                          C.POINTER(sz)]
     L.ladds_gpu_step.argtypes = [vp, i, vp, sz, C.POINTER(sz), C.POINTER(StepStats)]
+    L.ladds_population_write.argtypes = [C.c_char_p, sz] + [vp] * 12
+    L.ladds_population_read.argtypes = [C.c_char_p, sz, C.POINTER(sz)] + [vp] * 12
     L.ladds_gpu_step_host.argtypes = [vp, sz, C.POINTER(vp), C.POINTER(vp), vp, sz, C.POINTER(sz),
                                       C.POINTER(StepStats)]
     L.ladds_gpu_pending_records.argtypes = [vp, vp, sz, C.POINTER(sz)]
@@ -238,6 +241,27 @@ def generate_population(which: int, seed: int, n: int) -> dict:
     rc = lib().ladds_population_generate(which, seed, n, *[_p(pop[k]) for k in POP_FIELDS])
     if rc:
         raise LaddsError(rc, "population generation failed")
+    return pop
+
+
+def save_population(path: str, pop: dict):
+    """Writes a population as a binary SoA population file (ladds_population_write)."""
+    pop = as_population(pop)
+    rc = lib().ladds_population_write(os.fsencode(path), len(pop["x"]), *[_p(pop[k]) for k in POP_FIELDS])
+    if rc:
+        raise LaddsError(rc, f"cannot write population file {path}")
+
+
+def load_population(path: str) -> dict:
+    """Reads a binary SoA population file (ladds_population_read)."""
+    n = C.c_size_t()
+    rc = lib().ladds_population_read(os.fsencode(path), 0, C.byref(n), *([None] * 12))
+    if rc not in (OK, ERR_CAPACITY):
+        raise LaddsError(rc, f"not a population file: {path}")
+    pop = empty_population(n.value)
+    rc = lib().ladds_population_read(os.fsencode(path), n.value, C.byref(n), *[_p(pop[k]) for k in POP_FIELDS])
+    if rc:
+        raise LaddsError(rc, f"not a population file: {path}")
     return pop
 
 

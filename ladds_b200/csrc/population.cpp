@@ -11,6 +11,7 @@
 // rho = 2700 kg/m^3, aom = pi r^2 1e-6 / m [km^2/kg] (Particle.h:72),
 // bcInv = Cd pi r^2 / m with Cd = 2.2 (Particle.cpp:13-17).
 #include <cmath>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 
@@ -264,3 +265,79 @@ void adjointPairDraw(uint64_t seed, size_t p, double dt, int steps, double stA[6
 }
 
 }  // namespace ladds
+
+// ---- binary SoA population files ----
+//
+// One file holds a population for every consumer (the library, the oracle, the
+// benchmark): a 24-byte little-endian header {char magic[8] = "LADDSPOP",
+// u32 version = 1, u32 fields = 12, u64 n} followed by the twelve arrays of the
+// upload order, each n long: x, y, z, vx, vy, vz, radius, aom, bcInv (f64),
+// id, parentId (u64), activity (i8).
+namespace {
+constexpr char kPopMagic[8] = {'L', 'A', 'D', 'D', 'S', 'P', 'O', 'P'};
+constexpr uint32_t kPopVersion = 1, kPopFields = 12;
+
+struct PopHeader {
+  char magic[8];
+  uint32_t version, fields;
+  uint64_t n;
+};
+static_assert(sizeof(PopHeader) == 24, "population file header is 24 bytes");
+
+int readHeader(std::FILE *f, uint64_t *n) {
+  PopHeader h{};
+  if (std::fread(&h, sizeof(h), 1, f) != 1) return LADDS_ERR_INVALID_ARG;
+  if (std::memcmp(h.magic, kPopMagic, sizeof(kPopMagic)) != 0 || h.version != kPopVersion ||
+      h.fields != kPopFields)
+    return LADDS_ERR_INVALID_ARG;
+  *n = h.n;
+  return LADDS_OK;
+}
+}  // namespace
+
+extern "C" int ladds_population_write(const char *path, size_t n, const double *x, const double *y, const double *z,
+                                      const double *vx, const double *vy, const double *vz, const double *radius,
+                                      const double *aom, const double *bcInv, const uint64_t *id,
+                                      const uint64_t *parentId, const int8_t *activity) {
+  const void *arr[12] = {x, y, z, vx, vy, vz, radius, aom, bcInv, id, parentId, activity};
+  if (!path) return LADDS_ERR_INVALID_ARG;
+  for (const void *p : arr)
+    if (n && !p) return LADDS_ERR_INVALID_ARG;
+  std::FILE *f = std::fopen(path, "wb");
+  if (!f) return LADDS_ERR_INVALID_ARG;
+  PopHeader h{};
+  std::memcpy(h.magic, kPopMagic, sizeof(kPopMagic));
+  h.version = kPopVersion;
+  h.fields = kPopFields;
+  h.n = n;
+  bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+  for (int a = 0; a < 12 && ok && n; ++a) ok = std::fwrite(arr[a], a < 11 ? 8 : 1, n, f) == n;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? LADDS_OK : LADDS_ERR_INVALID_ARG;
+}
+
+extern "C" int ladds_population_read(const char *path, size_t cap, size_t *n, double *x, double *y, double *z,
+                                     double *vx, double *vy, double *vz, double *radius, double *aom, double *bcInv,
+                                     uint64_t *id, uint64_t *parentId, int8_t *activity) {
+  if (!path || !n) return LADDS_ERR_INVALID_ARG;
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) return LADDS_ERR_INVALID_ARG;
+  uint64_t count = 0;
+  int rc = readHeader(f, &count);
+  if (rc == LADDS_OK) {
+    *n = (size_t)count;
+    if (count > cap) rc = LADDS_ERR_CAPACITY;
+  }
+  void *arr[12] = {x, y, z, vx, vy, vz, radius, aom, bcInv, id, parentId, activity};
+  for (int a = 0; a < 12 && rc == LADDS_OK && count; ++a) {
+    const size_t size = a < 11 ? 8 : 1;
+    if (arr[a]) {
+      if (std::fread(arr[a], size, count, f) != count) rc = LADDS_ERR_INVALID_ARG;
+    } else if (std::fseek(f, (long)(size * count), SEEK_CUR) != 0) {
+      rc = LADDS_ERR_INVALID_ARG;
+    }
+  }
+  if (rc == LADDS_OK && std::fgetc(f) != EOF) rc = LADDS_ERR_INVALID_ARG;  // trailing bytes: not this format
+  std::fclose(f);
+  return rc;
+}
