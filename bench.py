@@ -207,15 +207,28 @@ def measured_peaks_file():
 
 
 # ------------------------------------------------------------- CPU baseline
-def cpu_baseline(n_objects, seed, budget_s=20.0, steps_cap=None):
+def bench_population(args, seed):
+    """The benchmark's population: the binary SoA population file given with
+    --population, else the seeded population 0 of --n-objects objects."""
+    from ladds_b200 import capi
+
+    if args.population:
+        return capi.load_population(args.population)
+    return capi.generate_population(0, seed, args.n_objects)
+
+
+def workload_name(args, n):
+    if args.population:
+        return (f"population file {os.path.basename(args.population)} ({n} objects), " + WORKLOAD.split(", ", 2)[2])
+    return WORKLOAD
+
+
+def cpu_baseline(pop, budget_s=20.0, steps_cap=None):
     """Times the oracle (C + OpenMP restatement of the reference path) on the host
     cores: full Yoshida step of the full force set + linked-cell scan."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
 
-    from ladds_b200 import capi
-
-    pop = capi.generate_population(0, seed, n_objects)
     opop = O.Population(pop["x"], pop["y"], pop["z"], pop["vx"], pop["vy"], pop["vz"], pop["radius"], pop["aom"],
                         pop["bc_inv"], pop["id"], pop["parent"], pop["activity"])
     grid = O.make_grid([-10000.0] * 3, [10000.0] * 3, 0.0, 80.0)
@@ -245,7 +258,7 @@ def run_reference(args, world, rank):
 
     from ladds_b200 import capi
 
-    pop = capi.generate_population(0, SEED, args.n_objects)
+    pop = bench_population(args, SEED)
     grid = O.make_grid([-10000.0] * 3, [10000.0] * 3, 0.0, 80.0)
     params = O.scan_params(cutoff=80.0, dt=10.0)
 
@@ -262,7 +275,7 @@ def run_reference(args, world, rank):
     per_obj = t_probe / max(probe.n, 1)
     budget = args.reference_budget
     m_target = budget / max(args.steps + args.warmup, 1) / per_obj
-    frac = min(1.0, max(m_target / args.n_objects, 1e-4))
+    frac = min(1.0, max(m_target / max(len(pop["x"]), 1), 1e-4))
     sample = to_o(wedge_population(pop, frac))
     for w in range(args.warmup):
         O.propagate(sample, O.FULL, 10.0, 1, t0=10.0 * w)
@@ -277,8 +290,10 @@ def run_reference(args, world, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / max(args.steps, 1),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_objects": args.n_objects, "sample_objects": sample.n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "population file" if args.population else "synthetic",
+        "config": {"workload": workload_name(args, len(pop["x"])), "n_objects": len(pop["x"]),
+                   "sample_objects": sample.n,
                    "sample": f"longitude wedge of {frac:.4f} of the population (same density)",
                    "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": "object-steps/s", "cores": cores, "kind": "port",
@@ -381,6 +396,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=16)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-objects", type=int, default=N_OBJECTS)
+    ap.add_argument("--population", default=None,
+                    help="binary SoA population file (ladds_population_write) instead of the seeded population 0")
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--no-drift", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -400,8 +417,8 @@ def main():
     from ladds_b200 import build, capi
 
     build.build_gpu()
-    n = args.n_objects
-    pop = capi.generate_population(0, SEED + rank, n)  # replicas: one population per rank
+    pop = bench_population(args, SEED + rank)  # replicas: one population per rank (or the file's)
+    n = len(pop["x"])
 
     def make_ctx(precision, graphs=1):
         return capi.Context(capi.default_config(componentMask=capi.PROP_ALL, precision=precision, device=local,
@@ -574,7 +591,7 @@ def main():
     cpu = None
     if not args.no_cpu and world == 1:
         try:
-            O, opop, grid, params, t_full, cores = cpu_baseline(n, SEED)
+            O, opop, grid, params, t_full, cores = cpu_baseline(bench_population(args, SEED))
             steps = max(1, int(args.cpu_budget / max(t_full, 1e-3)))
             t0 = time.perf_counter()
             for s in range(steps):
@@ -600,8 +617,8 @@ def main():
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64+f32 (split)",
-        "data": "synthetic (seeded population 0)",
-        "config": {"workload": WORKLOAD, "n_objects": n, "precision": "split", "dt_s": 10.0,
+        "data": "population file" if args.population else "synthetic (seeded population 0)",
+        "config": {"workload": workload_name(args, n), "n_objects": n, "precision": "split", "dt_s": 10.0,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2: per-step working set ~450 MB (state 2 x 92 MB + keys + packed)"},
         "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
