@@ -224,8 +224,10 @@ int ladds_gpu_step(ladds_gpu_ctx *ctx, int iterations, ladds_pair *out, size_t c
  * after the step (`outState` may be `in`: the update is then in place).  The
  * arrays cross PCIe in up to 4 chunks: a chunk is propagated as soon as it is
  * on the device and copied back while the next one comes in (both PCIe
- * directions at once; pinned host memory is needed for the copies to overlap).
- * The scan (when iteration % k == 0) follows the propagation.  The result equals ladds_gpu_set_state + ladds_gpu_step(1) +
+ * directions at once).  Pageable arrays go through a pinned staging buffer of
+ * the context (allocated on first use, 96 B per object), copied chunk by chunk
+ * on all host threads; pinned arrays (cudaHostAlloc / cudaHostRegister) are
+ * copied directly.  The scan (when iteration % k == 0) follows the propagation.  The result equals ladds_gpu_set_state + ladds_gpu_step(1) +
  * ladds_gpu_get_state, bit for bit.  LADDS_ERR_CAPACITY: the
  * iteration HAS been taken (outState holds its state), *nOut is the number of
  * records and ladds_gpu_pending_records returns them.  Other errors: the

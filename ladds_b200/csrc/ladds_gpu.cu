@@ -79,7 +79,9 @@ struct ladds_gpu_ctx {
   cudaStream_t st3 = nullptr;  // device-to-host copies of ladds_gpu_step_host
   cudaEvent_t evCells = nullptr, evScan = nullptr;
   cudaEvent_t evXfer[7] = {};  // per-array hand-offs between copies and (un)permutes of set/get_state
-  cudaEvent_t evPipe[2 * kHostChunks + 1] = {};  // chunk hand-offs of ladds_gpu_step_host
+  cudaEvent_t evPipe[3 * kHostChunks + 1] = {};  // chunk hand-offs of ladds_gpu_step_host
+  double *pinStage = nullptr;  // pinned staging of ladds_gpu_step_host for pageable arrays (12 x pinCap)
+  size_t pinCap = 0;
   std::vector<ladds_pair> pending;  // records of a ladds_gpu_step_host call whose buffer was too small
   int64_t *dIterBase = nullptr;  // first iteration of the chunk being run (device)
   size_t n = 0, cap = 0;
@@ -955,6 +957,7 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
     if (e) cudaEventDestroy(e);
   for (auto e : c->evPipe)
     if (e) cudaEventDestroy(e);
+  if (c->pinStage) cudaFreeHost(c->pinStage);
   if (c->st3) cudaStreamDestroy(c->st3);
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
@@ -1525,6 +1528,35 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
   return LADDS_OK;
 }
 
+}  // extern "C"
+
+namespace {
+constexpr size_t kHostCopyBlock = (size_t)1 << 17;  // doubles per task of the staging copies
+
+bool isPinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// dst[a][lo, lo + len) = src[a][lo, lo + len) for the arrays with use[a], on all host threads
+void hostCopy(double *const dst[6], const double *const src[6], const bool use[6], size_t lo, size_t len) {
+  const long per = (long)((len + kHostCopyBlock - 1) / kHostCopyBlock);
+#pragma omp parallel for schedule(static)
+  for (long t = 0; t < 6 * per; ++t) {
+    const int a = (int)(t / per);
+    if (!use[a]) continue;
+    const size_t b = lo + (size_t)(t % per) * kHostCopyBlock, e = std::min(b + kHostCopyBlock, lo + len);
+    std::memcpy(dst[a] + b, src[a] + b, (e - b) * sizeof(double));
+  }
+}
+}  // namespace
+
+extern "C" {
+
 int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], double *const outState[6],
                         ladds_pair *out, size_t cap, size_t *nOut, ladds_step_stats *stats) {
   if (!c || !in || !outState || !nOut) return LADDS_ERR_INVALID_ARG;
@@ -1554,6 +1586,37 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   }
   CK(enqueueEphemeris(c, 1));
   if (scan) CK(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
+  // pageable arrays go through pinned staging, copied on all host threads
+  // chunk by chunk (the driver's own staging of pageable copies is slower)
+  bool stageIn[6] = {}, stageOut[6] = {}, anyIn = false, anyOut = false;
+  for (int a = 0; a < 6 && n; ++a) {
+    stageIn[a] = !isPinned(in[a]);
+    stageOut[a] = !isPinned(outState[a]);
+    anyIn |= stageIn[a];
+    anyOut |= stageOut[a];
+  }
+  if ((anyIn || anyOut) && c->pinCap < n) {
+    if (c->pinStage) cudaFreeHost(c->pinStage);
+    c->pinStage = nullptr;
+    c->pinCap = 0;
+    if (cudaHostAlloc(&c->pinStage, 12 * n * sizeof(double), cudaHostAllocDefault) == cudaSuccess) {
+      c->pinCap = n;
+    } else {  // no pinned memory to spare: the driver stages the copies
+      cudaGetLastError();
+      c->pinStage = nullptr;
+      for (int a = 0; a < 6; ++a) stageIn[a] = stageOut[a] = false;
+      anyIn = anyOut = false;
+    }
+  }
+  double *pinIn[6], *pinOut[6];
+  const double *src[6];
+  double *dstHost[6];
+  for (int a = 0; a < 6; ++a) {
+    pinIn[a] = c->pinStage ? c->pinStage + (size_t)a * c->pinCap : nullptr;
+    pinOut[a] = c->pinStage ? c->pinStage + (size_t)(6 + a) * c->pinCap : nullptr;
+    src[a] = stageIn[a] ? pinIn[a] : in[a];
+    dstHost[a] = stageOut[a] ? pinOut[a] : outState[a];
+  }
   // chunks: host->device on st2, propagation on st, device->host on st3
   const int chunks = (int)std::max<size_t>(1, std::min<size_t>((size_t)kHostChunks, n / kHostChunkMin));
   const size_t per = (n + (size_t)chunks - 1) / (size_t)chunks;
@@ -1563,18 +1626,20 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     const size_t lo = (size_t)ch * per;
     if (lo >= n) break;
     const size_t len = std::min(per, n - lo);
+    if (anyIn) hostCopy(pinIn, in, stageIn, lo, len);
     for (int a = 0; a < 6; ++a)
-      CK(cudaMemcpyAsync(sArr[a] + lo, in[a] + lo, len * sizeof(double), cudaMemcpyHostToDevice, c->st2));
-    CK(cudaEventRecord(c->evPipe[2 * ch], c->st2));
-    CK(cudaStreamWaitEvent(c->st, c->evPipe[2 * ch], 0));
+      CK(cudaMemcpyAsync(sArr[a] + lo, src[a] + lo, len * sizeof(double), cudaMemcpyHostToDevice, c->st2));
+    CK(cudaEventRecord(c->evPipe[ch], c->st2));
+    CK(cudaStreamWaitEvent(c->st, c->evPipe[ch], 0));
     DevState Sc = S;
     Sc.x += lo; Sc.y += lo; Sc.z += lo; Sc.vx += lo; Sc.vy += lo; Sc.vz += lo;
     Sc.aom += lo; Sc.bc += lo; Sc.tag += lo;
     launchPropagate(c, Sc, (int)len, 1, 0, scan, c->keys0 + lo, c->scratchC + lo);
-    CK(cudaEventRecord(c->evPipe[2 * ch + 1], c->st));
-    CK(cudaStreamWaitEvent(c->st3, c->evPipe[2 * ch + 1], 0));
+    CK(cudaEventRecord(c->evPipe[kHostChunks + ch], c->st));
+    CK(cudaStreamWaitEvent(c->st3, c->evPipe[kHostChunks + ch], 0));
     for (int a = 0; a < 6; ++a)
-      CK(cudaMemcpyAsync(outState[a] + lo, sArr[a] + lo, len * sizeof(double), cudaMemcpyDeviceToHost, c->st3));
+      CK(cudaMemcpyAsync(dstHost[a] + lo, sArr[a] + lo, len * sizeof(double), cudaMemcpyDeviceToHost, c->st3));
+    CK(cudaEventRecord(c->evPipe[2 * kHostChunks + ch], c->st3));
     used = ch + 1;
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, 1);
@@ -1608,10 +1673,16 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     for (int a = 0; a < 6; ++a) k_permute_from_slots_f64<<<g, 256, 0, c->st>>>(sArr[a], c->cur.tag, ni, dst[a]);
   }
   if (used) {
-    CK(cudaEventRecord(c->evPipe[2 * kHostChunks], c->st3));
-    CK(cudaStreamWaitEvent(c->st, c->evPipe[2 * kHostChunks], 0));
+    CK(cudaEventRecord(c->evPipe[3 * kHostChunks], c->st3));
+    CK(cudaStreamWaitEvent(c->st, c->evPipe[3 * kHostChunks], 0));
   }
   CK(cudaEventRecord(c->callEnd, c->st));
+  // staged outputs: each chunk leaves the pinned buffer as soon as it is there
+  for (int ch = 0; ch < used && anyOut; ++ch) {
+    CK(cudaEventSynchronize(c->evPipe[2 * kHostChunks + ch]));
+    const size_t lo = (size_t)ch * per;
+    hostCopy(outState, pinOut, stageOut, lo, std::min(per, n - lo));
+  }
   auto undo = [&](int rc) {
     // the iteration is not counted; the device copy of the state is replaced by
     // the next call's host state

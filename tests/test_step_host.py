@@ -145,3 +145,24 @@ def test_step_host_rejects_bad_arguments(capi):
         with pytest.raises(ValueError):
             ctx.step_host([pop["x"][:10]] * 6)
         assert ctx.iteration() == 0
+
+
+def test_step_host_mixed_pinned_and_pageable(capi):
+    """Each array on its own: pageable ones go through the pinned staging."""
+    pop = capi.generate_population(0, 2032, 300_000)
+    kw = dict(componentMask=capi.PROP_ALL, conjunctionThreshold=10.0)
+    names = ("x", "y", "z", "vx", "vy", "vz")
+    with capi.Context(capi.default_config(**kw)) as a, capi.Context(capi.default_config(**kw)) as b:
+        a.upload(pop)
+        b.upload(pop)
+        pinned = pinned_state([pop[f] for f in names])
+        host_in = pinned[:3] + [np.array(pop[f]) for f in names[3:]]
+        for it in range(2):
+            a.set_state(*host_in)
+            ra = a.step(1)
+            out = [np.zeros(len(pop["x"])) for _ in range(3)] + pinned_state([np.zeros(len(pop["x"]))] * 3)
+            rb = b.step_host(host_in, out)
+            for x, y in zip(a.get_state(), out):
+                assert np.array_equal(x, y), f"state differs at iteration {it}"
+            assert records_equal(ra.records, rb.records), describe_diff(ra.records, rb.records)
+            host_in = out
