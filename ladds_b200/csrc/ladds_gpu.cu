@@ -1587,7 +1587,7 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   CK(enqueueEphemeris(c, 1));
   if (scan) CK(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
   // pageable arrays go through pinned staging, copied on all host threads
-  // chunk by chunk (the driver's own staging of pageable copies is slower)
+  // chunk by chunk (the CUDA driver's own staging of pageable copies is slower)
   bool stageIn[6] = {}, stageOut[6] = {}, anyIn = false, anyOut = false;
   for (int a = 0; a < 6 && n; ++a) {
     stageIn[a] = !isPinned(in[a]);
@@ -1601,7 +1601,7 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     c->pinCap = 0;
     if (cudaHostAlloc(&c->pinStage, 12 * n * sizeof(double), cudaHostAllocDefault) == cudaSuccess) {
       c->pinCap = n;
-    } else {  // no pinned memory to spare: the driver stages the copies
+    } else {  // no pinned memory to spare: the CUDA driver stages the copies
       cudaGetLastError();
       c->pinStage = nullptr;
       for (int a = 0; a < 6; ++a) stageIn[a] = stageOut[a] = false;

@@ -2,8 +2,8 @@
  * ladds_oracle.h -- CPU oracle for the LADDS propagate + conjunction hot path.
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
- * calls this code.  It is used by tests/ (as the checker), by
- * __graft_entry__.smoke() (as the checker) and by bench.py's cpu_baseline /
+ * calls this code.  It is used by tests/ and __graft_entry__.smoke() to check
+ * the GPU results, and by bench.py's cpu_baseline /
  * --impl reference leg (as the timed CPU restatement of the reference path).
  *
  * What it restates (reference paths relative to the esa/LADDS tree):

@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (liboracle.so).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` as
-the checker and by ``bench.py``'s CPU-baseline leg.  The product library never
+TEST INFRASTRUCTURE ONLY: imported by tests/ and ``__graft_entry__.smoke()`` to
+check the GPU results, and by ``bench.py``'s CPU-baseline leg.  The product library never
 imports this module.  See ``ladds_oracle.h`` for what each function restates
 and for its parity status.
 """

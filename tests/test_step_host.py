@@ -42,7 +42,7 @@ def run_pair(capi, pop, iters, precision, k=1, pair_cap=1 << 16, in_place=True, 
         if pre:  # graph-replayed iterations first: step_host must keep the buffer roles they were made with
             assert records_equal(a.step(pre).records, b.step(pre).records)
             pop = dict(zip(("x", "y", "z", "vx", "vy", "vz"), a.get_state()))
-        # pinned: asynchronous copies that overlap; pageable: staged by the driver
+        # pinned: asynchronous copies that overlap; pageable: staged by the library
         stage = pinned_state if pinned else (lambda arrays: [np.array(a, dtype=np.float64) for a in arrays])
         host = stage([pop[f] for f in ("x", "y", "z", "vx", "vy", "vz")])
         total = 0
