@@ -57,6 +57,13 @@ class GpuContext {
   // the container last uploaded (pointer + size), to detect host-side changes
   bool mirrors(const Container &container) const;
   void markMirrored(const Container &container);
+  // forgets the mirror, so that the next call uploads the container again:
+  // needed after particles were changed in place with the size unchanged
+  // (e.g. two removed and two appended), which the pointer + size test misses
+  void invalidate() {
+    mirror_ = nullptr;
+    mirrorSize_ = 0;
+  }
 
  private:
   ladds_gpu_config cfg_;

@@ -4,10 +4,12 @@
 // The acceleration components are the reference's std::array<bool, 8> mask
 // (KEP, J2, C22, S22, SOL, LUN, SRP, DRAG; Simulation.cpp:127-135) plus J3.
 // integrate() runs one Yoshida-4 step of every particle on the GPU.  In the
-// host-owned mode (default) the container is uploaded when it changed and the
-// new positions / velocities are written back after every step, as the
-// reference integrator updates the particles in place; in the device-resident
-// mode the state stays on the GPU until sync().
+// host-owned mode (default) the container is uploaded when it changed (another
+// container, or another size; after changing particles in place at the same
+// size call GpuContext::invalidate()) and the new positions / velocities are
+// written back after every step, as the reference integrator updates the
+// particles in place; in the device-resident mode the state stays on the GPU
+// until sync().
 #pragma once
 #include <array>
 
