@@ -188,6 +188,21 @@ static void gpuTests() {
     const double moved = std::sqrt(dx * dx + dy * dy + dz * dz);
     CHECK(moved > 7.0 && moved < 8.0);
   }
+  // GpuContext::invalidate(): a particle changed in place (same container, same
+  // size) reaches the device on the next step
+  {
+    auto cfg = ladds::ConfigReader::fromString(kSimConfig);
+    ladds::GpuContext gpu(ladds::GpuContext::configFrom(cfg));
+    ladds::Container c;
+    c.push_back(mk({6871., 0., 0.}, {0., 4.8958309146899, 5.83462408131549}, 1, AS::passive, 1.));
+    ladds::Integrator integ(c, gpu);
+    integ.integrate(false);
+    c[0].setR({-6871., 0., 0.});  // the other side of the Earth
+    c[0].setV({0., -4.8958309146899, -5.83462408131549});
+    gpu.invalidate();
+    integ.integrate(false);
+    CHECK(c[0].getR()[0] < -6800.);  // stepped from the new state, not from the device's old one
+  }
 }
 
 int main(int argc, char **argv) {
