@@ -210,17 +210,24 @@ def measured_peaks_file():
 def bench_population(args, seed):
     """The benchmark's population: the binary SoA population file given with
     --population, else the seeded population 0 of --n-objects objects."""
-    from ladds_b200 import capi
+    from ladds_b200 import population  # host-only library: no GPU code in the process
 
     if args.population:
-        return capi.load_population(args.population)
-    return capi.generate_population(0, seed, args.n_objects)
+        return population.load_population(args.population)
+    return population.generate_population(0, seed, args.n_objects)
 
 
 def workload_name(args, n):
     if args.population:
         return (f"population file {os.path.basename(args.population)} ({n} objects), " + WORKLOAD.split(", ", 2)[2])
     return WORKLOAD
+
+
+def bench_config(args, n):
+    """The workload both arms print, key for key: what is computed, not how."""
+    return {"workload": workload_name(args, n), "n_objects": n, "dt_s": 10.0, "scan_every_steps": 1,
+            "cutoff_km": 80.0, "conjunction_threshold_km": 0.1,
+            "forces": "KEP J2 J3 C22 S22 SOL LUN SRP DRAG"}
 
 
 def cpu_baseline(pop, budget_s=20.0, steps_cap=None):
@@ -256,8 +263,6 @@ def run_reference(args, world, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
 
-    from ladds_b200 import capi
-
     pop = bench_population(args, SEED)
     grid = O.make_grid([-10000.0] * 3, [10000.0] * 3, 0.0, 80.0)
     params = O.scan_params(cutoff=80.0, dt=10.0)
@@ -291,20 +296,20 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "population file" if args.population else "synthetic",
-        "config": {"workload": workload_name(args, len(pop["x"])), "n_objects": len(pop["x"]),
-                   "sample_objects": sample.n,
-                   "sample": f"longitude wedge of {frac:.4f} of the population (same density)",
-                   "l2": "n/a (CPU)"},
+        "data": "population file" if args.population else "synthetic (seeded population 0)",
+        "config": bench_config(args, len(pop["x"])),
+        "parallelism": "1 process, OpenMP",
+        "l2": "n/a (CPU)",
         "cpu_baseline": {"value": value, "unit": "object-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample.n} objects (longitude wedge, same density) x {args.steps} steps"},
+                         "sample": f"{sample.n} objects (longitude wedge of {frac:.4f} of the population, same "
+                                   f"density) x {args.steps} steps per timed step"},
         "e2e": {"value": value, "unit": "object-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------ other workloads
-def workload_leg(capi, device, which, n, steps, tune, breakup_steps=0):
+def workload_leg(capi, device, which, n, steps, tune):
     """Throughput of population `which` (2: four constellation shells + debris,
     4: small-debris mixture) with the full force set in split precision, scan
     every step; optionally autotuned first (cell edge, block shapes, chunk)."""
@@ -323,19 +328,160 @@ def workload_leg(capi, device, which, n, steps, tune, breakup_steps=0):
         ms = res.stats.deviceMs
         out.update({"value": n * steps / (ms * 1e-3), "unit": "object-steps/s", "ms_per_step": ms / steps,
                     "records": int(res.stats.records), "collisions": int(res.stats.collisions)})
-        if breakup_steps:
-            # breakups on the host after every iteration, fragments appended on the device
-            cfg = capi.BreakupConfig(0.05, 1, 2.2)
-            next_id = n
-            total_b = total_f = 0
-            for it in range(breakup_steps):
-                r = ctx.step(1)
-                nb, nf, next_id = ctx.breakup(r.records, cfg, 1000 + it, next_id)
-                total_b += nb
-                total_f += nf
-            out["breakup_run"] = {"iterations": breakup_steps, "breakups": total_b, "fragments": total_f,
-                                  "objects_after": ctx.size()}
     return out
+
+
+# ------------------------------------------------------------ drift legs
+def closest_approach(ri, vi, rj, vj, dt):
+    """Distance at the endpoint and least distance of the straight segments
+    back-extrapolated over [-dt, 0] (the geometry of
+    DistanceApproximation.cpp:13-58, in numpy binary64; for classifying
+    differing records, not for parity)."""
+    dr, dv = ri - rj, vi - vj
+    o = dr - dv * dt
+    dv2 = np.sum(dv * dv, axis=-1)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t = np.clip(-np.sum(o * dv, axis=-1) / dv2, 0.0, dt)
+    t = np.where(np.isfinite(t), t, 0.0)
+    m = o + dv * t[..., None]
+    return np.sqrt(np.sum(dr * dr, axis=-1)), np.sqrt(np.sum(m * m, axis=-1))
+
+
+def objects_at_steps(capi, cfg, pop, wanted):
+    """{(step, slot): (r, v)}: the states of the wanted (step, slot) pairs, by
+    re-running the population from its start and stopping after each wanted
+    step (a record of step s is scanned on the state after s + 1 iterations)."""
+    out = {}
+    by_step = {}
+    for s_, sl in wanted:
+        by_step.setdefault(s_, set()).add(sl)
+    with capi.Context(cfg) as ctx:
+        ctx.upload(pop)
+        done = 0
+        for s_ in sorted(by_step):
+            if s_ + 1 > done:
+                ctx.step(s_ + 1 - done)
+                done = s_ + 1
+            slots = np.array(sorted(by_step[s_]), dtype=np.uint32)
+            objs = ctx.get_objects(slots)
+            for sl, o in zip(slots, objs):
+                out[(s_, int(sl))] = (np.array(o["r"]), np.array(o["v"]), float(o["radius"]), int(o["activity"]))
+    return out
+
+
+def classify_differences(capi, cfgs, pop, recs, dt):
+    """Each record that only one precision lists: the pair's own split-vs-FP64
+    difference at that step (states re-run to that step in both precisions)
+    against its margin to the threshold it crosses.  A record is explained when
+    the threshold or the cutoff lies within the pair's drift bound
+    |dr_A| + |dr_B| + dt (|dv_A| + |dv_B|) of its distance."""
+    key = lambda r: (int(r["step"]), int(r["idA"]), int(r["idB"]), int(r["flags"]) & 7)
+    ka = {key(r): r for r in recs["split"]}
+    kb = {key(r): r for r in recs["fp64"]}
+    diff = [(k, ka.get(k, kb.get(k))) for k in sorted(set(ka) ^ set(kb))]
+    if not diff:
+        return {"records_only_in_one": 0, "explained": 0}
+    wanted = set()
+    for _, r in diff:
+        wanted.add((int(r["step"]), int(r["slotA"])))
+        wanted.add((int(r["step"]), int(r["slotB"])))
+    st = {name: objects_at_steps(capi, cfgs[name], pop, wanted) for name in ("split", "fp64")}
+    cfg = cfgs["fp64"]
+    rows = []
+    for k, r in diff:
+        s_, a, b = int(r["step"]), int(r["slotA"]), int(r["slotB"])
+        (ra, va, rad_a, act_a), (rb, vb, rad_b, act_b) = st["split"][(s_, a)], st["split"][(s_, b)]
+        (ra2, va2, _, _), (rb2, vb2, _, _) = st["fp64"][(s_, a)], st["fp64"][(s_, b)]
+        bound = (np.linalg.norm(ra - ra2) + np.linalg.norm(rb - rb2)
+                 + dt * (np.linalg.norm(va - va2) + np.linalg.norm(vb - vb2)))
+        d1, dl1 = closest_approach(ra, va, rb, vb, dt)
+        d2, dl2 = closest_approach(ra2, va2, rb2, vb2, dt)
+        thr = [cfg.conjunctionThreshold, cfg.evasionCutoff,
+               (rad_a + rad_b) * cfg.collisionDistanceFactor / 1000.0]
+        margins = [(abs(dl1 - t), t) for t in thr] + [(abs(d1 - cfg.cutoff), cfg.cutoff)]
+        m, t = min(margins)
+        rows.append({"step": s_, "in": "split" if k in ka else "fp64", "margin_km": float(m), "threshold_km": t,
+                     "bound_km": float(bound), "dl_split_km": float(dl1), "dl_fp64_km": float(dl2),
+                     "straddles": bool(min(dl1, dl2) - 1e-12 <= t <= max(dl1, dl2) + 1e-12
+                                       or min(d1, d2) - 1e-12 <= t <= max(d1, d2) + 1e-12)})
+    explained = [x for x in rows if x["margin_km"] <= x["bound_km"] * (1 + 1e-6) + 1e-12]
+    return {"records_only_in_one": len(rows), "explained": len(explained),
+            "straddling_a_threshold": sum(x["straddles"] for x in rows),
+            "max_margin_m": max(x["margin_km"] for x in rows) * 1e3,
+            "max_margin_rel": max(x["margin_km"] / x["threshold_km"] for x in rows),
+            "max_pair_drift_bound_m": max(x["bound_km"] for x in rows) * 1e3,
+            "first_step": min(x["step"] for x in rows), "examples": rows[:3]}
+
+
+def drift_leg(capi, device, pop, steps, cfg_kw=None):
+    """Split vs FP64 from the same start over `steps` iterations (scan every
+    iteration): RMS / max position difference at the end, record counts, and
+    the records that only one precision lists, classified."""
+    cfg_kw = dict(cfg_kw or {})
+    cfgs = {name: capi.default_config(componentMask=capi.PROP_ALL, precision=prec, device=device,
+                                      pairCapacity=1 << 18, **cfg_kw)
+            for name, prec in (("split", capi.PRECISION_SPLIT), ("fp64", capi.PRECISION_FP64))}
+    finals, recs, ms = {}, {}, {}
+    for name in ("split", "fp64"):
+        with capi.Context(cfgs[name]) as ctx:
+            ctx.upload(pop)
+            r = ctx.step(steps)
+            d = ctx.download()
+            finals[name] = (np.stack([d["x"], d["y"], d["z"]], 1), np.stack([d["vx"], d["vy"], d["vz"]], 1))
+            recs[name] = r.records
+            ms[name] = r.stats.deviceMs
+    dr = finals["split"][0] - finals["fp64"][0]
+    dv = finals["split"][1] - finals["fp64"][1]
+    dt = cfgs["fp64"].deltaT
+    out = {"n_objects": len(pop["x"]), "steps": steps, "hours": steps * dt / 3600.0,
+           "rms_m": float(np.sqrt(np.mean(np.sum(dr * dr, 1)))) * 1e3,
+           "max_m": float(np.max(np.linalg.norm(dr, axis=1)) * 1e3),
+           "max_dv_mm_s": float(np.max(np.linalg.norm(dv, axis=1)) * 1e6),
+           "records_split": len(recs["split"]), "records_fp64": len(recs["fp64"]),
+           "ms_per_step_split": ms["split"] / steps, "ms_per_step_fp64": ms["fp64"] / steps}
+    out["differences"] = classify_differences(capi, cfgs, pop, recs, dt)
+    return out
+
+
+def breakup_leg(capi, device, pop, iterations, cfg_kw):
+    """Config 4 form: every iteration one ladds_gpu_step(1), then the NASA
+    breakup model on the host for the iteration's collision records, the
+    fragments appended on the device (BreakupWrapper.cpp:13-45,
+    Simulation.cpp:610-633).  Also the expected collision rate of the
+    conjunction records, sum of ((r_A + r_B) / 0.1 km)^2 over them (the
+    fraction of a uniform-in-area miss distribution inside the collision
+    radius)."""
+    cfg = capi.default_config(componentMask=capi.PROP_ALL, precision=capi.PRECISION_SPLIT, device=device,
+                              pairCapacity=1 << 18, **cfg_kw)
+    bcfg = capi.BreakupConfig(0.05, 1, 2.2)
+    radius = pop["radius"]
+    n = len(pop["x"])
+    next_id = int(np.max(pop["id"])) + 1 if n else 0
+    tot = dict(breakups=0, fragments=0, collisions=0, conjunctions=0)
+    expected = 0.0
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    with capi.Context(cfg) as ctx:
+        ctx.upload(pop)
+        for it in range(iterations):
+            r = ctx.step(1)
+            dev_ms += r.stats.deviceMs
+            rec = r.records
+            tot["collisions"] += int(r.stats.collisions)
+            conj = rec[(rec["flags"] & capi.PAIR_CONJUNCTION) != 0]
+            tot["conjunctions"] += len(conj)
+            sa, sb = conj["slotA"].astype(np.int64), conj["slotB"].astype(np.int64)
+            ok = (sa < n) & (sb < n)  # fragments (slots >= n) carry their own radii; the original ones suffice here
+            expected += float(np.sum(((radius[sa[ok]] + radius[sb[ok]]) * 1e-3 / 0.1) ** 2))
+            if r.stats.collisions:
+                nb, nf, next_id = ctx.breakup(rec, bcfg, 1000 + it, next_id)
+                tot["breakups"] += nb
+                tot["fragments"] += nf
+        size = ctx.size()
+    wall = time.perf_counter() - t0
+    return {"iterations": iterations, "hours": iterations * cfg.deltaT / 3600.0, **tot,
+            "expected_collisions_from_conjunctions": expected, "objects_after": size,
+            "ms_per_iteration_wall": wall * 1e3 / iterations, "ms_per_iteration_device": dev_ms / iterations}
 
 
 # ---------------------------------------------------------- adjoint leg
@@ -403,6 +549,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-workloads", action="store_true")
+    ap.add_argument("--drift-steps-8m", type=int, default=STEPS_PER_DAY // 3,
+                    help="iterations of the split-vs-FP64 comparison on the 8e6 population (0: skip)")
+    ap.add_argument("--breakup-steps", type=int, default=STEPS_PER_DAY,
+                    help="iterations of the 8e6 breakup run (host breakups, device append; 0: skip)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--reference-budget", type=float, default=150.0)
     args = ap.parse_args()
@@ -451,14 +601,13 @@ def main():
 
     workloads = {}
     if not args.no_workloads and rank == 0:
-        for name, which, n_obj, steps, tune, brk in (("constellation_shells", 2, 2_004_224, 128, True, 0),
-                                                      ("scale_8M", 4, 8_000_000, 32, True, 16)):
+        for name, which, n_obj, steps, tune in (("constellation_shells", 2, 2_004_224, 128, True),
+                                                ("scale_8M", 4, 8_000_000, 32, True)):
             try:
-                workloads[name] = workload_leg(capi, local, which, n_obj, steps, tune, brk)
+                workloads[name] = workload_leg(capi, local, which, n_obj, steps, tune)
             except Exception as ex:  # noqa: BLE001
                 workloads[name] = {"error": str(ex)[:200]}
 
-    # one-day drift of split vs FP64 (both from the same start state)
     adjoint = None
     if not args.no_adjoint and rank == 0:
         try:
@@ -467,23 +616,37 @@ def main():
             adjoint = {"error": str(ex)[:200]}
             print(f"adjoint leg failed: {ex}", file=sys.stderr)
 
-    drift = None
+    # split vs FP64 from the same start, per population: the benchmark's own
+    # population over one day, the constellation population over one day, the
+    # 8e6 scale population (in its autotuned cell form) over --drift-steps-8m
+    drift = {}
+    scale_kw = {}
+    tuned = workloads.get("scale_8M", {}).get("autotuned")
+    if tuned:
+        scale_kw = {k: tuned[k] for k in ("cellSize", "scanScreen", "propagateBlock", "scanBlock")}
     if not args.no_drift and rank == 0:
-        finals = {}
-        for name, prec in (("split", capi.PRECISION_SPLIT), ("fp64", capi.PRECISION_FP64)):
-            ctx = make_ctx(prec)
-            ctx.upload(pop)
-            r = ctx.step(STEPS_PER_DAY)
-            d = ctx.download()
-            finals[name] = (np.stack([d["x"], d["y"], d["z"]], 1), r.records)
-            ctx.close()
-        dr = finals["split"][0] - finals["fp64"][0]
-        rms_m = float(np.sqrt(np.mean(np.sum(dr * dr, 1)))) * 1e3
-        key = lambda recs: set(zip(recs["step"].tolist(), recs["idA"].tolist(), recs["idB"].tolist(),
-                                   (recs["flags"] & 7).tolist()))
-        a, b = key(finals["split"][1]), key(finals["fp64"][1])
-        drift = {"rms_m_one_day": rms_m, "max_m_one_day": float(np.max(np.linalg.norm(dr, axis=1)) * 1e3),
-                 "records_split": len(a), "records_fp64": len(b), "records_only_in_one": len(a ^ b)}
+        for name, mk_pop, steps, kw in (
+                ("population0_1e6", lambda: pop, STEPS_PER_DAY, {}),
+                ("constellation_shells_2e6", lambda: capi.generate_population(2, SEED + 2, 2_004_224),
+                 STEPS_PER_DAY, {}),
+                ("scale_8e6", lambda: capi.generate_population(4, SEED + 4, 8_000_000), args.drift_steps_8m,
+                 scale_kw)):
+            if steps <= 0:
+                continue
+            try:
+                drift[name] = drift_leg(capi, local, mk_pop(), steps, kw)
+            except Exception as ex:  # noqa: BLE001
+                drift[name] = {"error": str(ex)[:200]}
+                print(f"drift leg {name} failed: {ex}", file=sys.stderr)
+
+    breakups = None
+    if not args.no_workloads and rank == 0 and args.breakup_steps > 0:
+        try:
+            breakups = breakup_leg(capi, local, capi.generate_population(4, SEED + 4, 8_000_000),
+                                   args.breakup_steps, scale_kw)
+        except Exception as ex:  # noqa: BLE001
+            breakups = {"error": str(ex)[:200]}
+            print(f"breakup leg failed: {ex}", file=sys.stderr)
 
     # end to end through the C ABI, host-owned container: H2D state, step, D2H state + records
     e2e = None
@@ -605,6 +768,28 @@ def main():
 
     # kernels per step from the profiled run, + one ephemeris kernel per 128-step chunk
     launches_per_step = sum(split["phases"]["launches"].values()) / split["phases"]["steps"]
+    # the precision split changes the propagation only: the step-level ratio
+    # cannot exceed the FP64 step over its non-propagation part
+    fp64_per = {k: fp64_ph[k] / fp64_ph["steps"] for k in capi.PhaseTimes.PHASES}
+    shared_ms = max(sum(fp64_per.values()) - fp64_per["propagate"], 1e-9)
+    north = {
+        "mixed_over_fp64": value / fp64_value,
+        "fp64_value": fp64_value,
+        "propagate_fp64_over_split": fp64_per["propagate"] / max(per["propagate"], 1e-12),
+        "mixed_over_fp64_bound_propagation_free": sum(fp64_per.values()) / shared_ms,
+        "drift": {k: ({"steps": v["steps"], "rms_m": round(v["rms_m"], 5), "max_m": round(v["max_m"], 4),
+                       "records": [v["records_split"], v["records_fp64"]],
+                       "only_in_one": v["differences"]["records_only_in_one"],
+                       "explained": v["differences"]["explained"],
+                       "max_margin_m": v["differences"].get("max_margin_m")} if "error" not in v else v)
+                  for k, v in drift.items()},
+        "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
+        "adjoint_fd": (adjoint or {}).get("fd_summary"),
+        "breakups_8e6": ({k: breakups[k] for k in ("iterations", "collisions", "breakups", "fragments",
+                                                    "expected_collisions_from_conjunctions")}
+                         if breakups and "error" not in breakups else breakups),
+        "value_over_cpu_baseline": value / cpu["value"] if cpu and cpu.get("value") else None,
+    }
     line = {
         "metric": METRIC,
         "value": value,
@@ -618,23 +803,24 @@ def main():
         "vs_baseline": None,
         "dtype": "f64+f32 (split)",
         "data": "population file" if args.population else "synthetic (seeded population 0)",
-        "config": {"workload": workload_name(args, n), "n_objects": n, "precision": "split", "dt_s": 10.0,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2: per-step working set ~450 MB (state 2 x 92 MB + keys + packed)"},
-        "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
-        "mixed_over_fp64": value / fp64_value,
-        "drift": drift,
-        "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
-        "adjoint": adjoint,
+        "config": bench_config(args, n),
+        "precision": "split (FP64 central, J2, accumulation; FP32 J3, C22/S22, Sun, Moon, SRP, drag)",
+        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+        "l2": "inputs larger than L2: per-step working set ~450 MB (state 2 x 92 MB + keys + packed)",
+        "kernels": kernels,
         "workloads": workloads,
+        "adjoint": adjoint,
+        "drift": drift,
+        "breakups": breakups,
         "records": {"split": split["records"], "fp64": fp64["records"]},
+        "wall_s": {"split": split["wall"], "fp64": fp64["wall"]},
         "e2e": e2e,
         "roofline": roofline,
-        "kernels": kernels,
         "cpu_baseline": cpu,
         "clocks": split["clocks"],
         "gpu_launches": int(round(launches_per_step * args.steps)) + (args.steps + 127) // 128,
-        "wall_s": {"split": split["wall"], "fp64": fp64["wall"]},
+        "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
+        "north_star": north,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -319,7 +319,10 @@ int ladds_gpu_grid(const ladds_gpu_ctx *ctx, int32_t dims[3], int32_t *reach, do
  *                               sort by (key, j), the order of the contexts' scans,
  *   rowStart      (device, ny*nz + 1 entries, may be NULL) first position of
  *                               every cell row (iz, iy), then n.
- * Returns once the sort has finished (it synchronises `stream`).  Its scratch
+ * Returns once the sort has finished (it synchronises `stream`, so a stream
+ * that is capturing is refused with LADDS_ERR_INVALID_ARG; an error that earlier
+ * work left pending in the calling thread is reported as LADDS_ERR_CUDA and
+ * left in place, not cleared).  Its scratch
  * is one fixed device array of about 4 MB per device, sized for at most
  * LADDS_NOALLOC_SORT_MAX_OBJECTS objects and LADDS_NOALLOC_SORT_MAX_ROWS rows
  * (ny * nz); larger inputs return LADDS_ERR_TOO_LARGE with a message.  Keys

@@ -2,6 +2,9 @@
 
 * ``ladds_b200/libladds_gpu.so`` -- the sm_100a CUDA kernels and the C ABI of
   ``include/ladds_gpu.h`` (nvcc, ``-gencode arch=compute_100a,code=sm_100a``).
+* ``ladds_b200/libladds_population.so`` -- the seeded population generator
+  and the population file format alone (g++, no CUDA), for processes that
+  must not load GPU code.
 * ``ladds_b200/host/libladds_host.so`` -- the C++17 host mirror of the
   reference interface (ladds::Particle, ladds::Integrator,
   ladds::GpuCollisionFunctor, ladds::ConfigReader) on top of the C ABI.
@@ -69,6 +72,26 @@ def build_gpu(force: bool = False, verbose: bool = False, ptxas_info: bool = Fal
     return GPU_LIB
 
 
+POP_LIB = os.path.join(PKG, "libladds_population.so")
+
+
+def build_population(force: bool = False, verbose: bool = False) -> str:
+    """population.cpp alone as a host library (g++, no CUDA runtime)."""
+    srcs = [os.path.join(CSRC, "population.cpp")]
+    deps = srcs + [os.path.join(CSRC, "population.h"), os.path.join(CSRC, "physics.cuh"),
+                   os.path.join(ROOT, "include", "ladds_gpu.h")]
+    if not force and _newer(POP_LIB, deps):
+        return POP_LIB
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-o", POP_LIB, *srcs]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + r.stdout + r.stderr)
+    return POP_LIB
+
+
 PEAKS_LIB = os.path.join(PKG, "libladds_peaks.so")
 
 
@@ -128,6 +151,7 @@ def build_host_tests(force: bool = False, verbose: bool = False) -> str:
 
 def build(force: bool = False, verbose: bool = False) -> None:
     build_gpu(force=force, verbose=verbose)
+    build_population(force=force, verbose=verbose)
     build_peaks(force=force, verbose=verbose)
     build_host(force=force, verbose=verbose)
     build_host_tests(force=force, verbose=verbose)

@@ -33,10 +33,7 @@ PAIR_DTYPE = np.dtype([("idA", "<u8"), ("idB", "<u8"), ("slotA", "<u4"), ("slotB
 assert PAIR_DTYPE.itemsize == 64
 
 
-class LaddsError(RuntimeError):
-    def __init__(self, code, msg):
-        super().__init__(f"ladds_gpu error {code}: {msg}")
-        self.code = code
+from .population import LaddsError  # noqa: E402  (one error type for both libraries)
 
 
 class GpuConfig(C.Structure):
@@ -209,69 +206,27 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-POP_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "radius", "aom", "bc_inv", "id", "parent", "activity")
-_POP_DTYPES = dict(x=np.float64, y=np.float64, z=np.float64, vx=np.float64, vy=np.float64, vz=np.float64,
-                   radius=np.float64, aom=np.float64, bc_inv=np.float64, id=np.uint64, parent=np.uint64,
-                   activity=np.int8)
-
-
-def empty_population(n: int) -> dict:
-    return {k: np.zeros(n, dtype=t) for k, t in _POP_DTYPES.items()}
-
-
-def as_population(d: dict) -> dict:
-    out = {}
-    n = len(d["x"])
-    for k, t in _POP_DTYPES.items():
-        if k in d and d[k] is not None:
-            out[k] = np.ascontiguousarray(d[k], dtype=t)
-        elif k == "parent":
-            out[k] = np.full(n, SIZE_MAX, dtype=np.uint64)
-        elif k == "activity":
-            out[k] = np.zeros(n, dtype=np.int8)
-        elif k == "id":
-            out[k] = np.arange(n, dtype=np.uint64)
-        else:
-            raise KeyError(k)
-    return out
+from .population import POP_FIELDS, as_population, empty_population  # noqa: E402,F401
+from . import population as _population  # noqa: E402
 
 
 def generate_population(which: int, seed: int, n: int) -> dict:
-    pop = empty_population(n)
-    rc = lib().ladds_population_generate(which, seed, n, *[_p(pop[k]) for k in POP_FIELDS])
-    if rc:
-        raise LaddsError(rc, "population generation failed")
-    return pop
+    """Seeded population `which` of n objects (host library, no GPU code)."""
+    return _population.generate_population(which, seed, n)
 
 
 def save_population(path: str, pop: dict):
     """Writes a population as a binary SoA population file (ladds_population_write)."""
-    pop = as_population(pop)
-    rc = lib().ladds_population_write(os.fsencode(path), len(pop["x"]), *[_p(pop[k]) for k in POP_FIELDS])
-    if rc:
-        raise LaddsError(rc, f"cannot write population file {path}")
+    _population.save_population(path, pop)
 
 
 def load_population(path: str) -> dict:
     """Reads a binary SoA population file (ladds_population_read)."""
-    n = C.c_size_t()
-    rc = lib().ladds_population_read(os.fsencode(path), 0, C.byref(n), *([None] * 12))
-    if rc not in (OK, ERR_CAPACITY):
-        raise LaddsError(rc, f"not a population file: {path}")
-    pop = empty_population(n.value)
-    rc = lib().ladds_population_read(os.fsencode(path), n.value, C.byref(n), *[_p(pop[k]) for k in POP_FIELDS])
-    if rc:
-        raise LaddsError(rc, f"not a population file: {path}")
-    return pop
+    return _population.load_population(path)
 
 
 def elements_to_state(a, e, inc, raan, argp, M):
-    r = np.zeros(3)
-    v = np.zeros(3)
-    rc = lib().ladds_elements_to_state(a, e, inc, raan, argp, M, _p(r), _p(v))
-    if rc:
-        raise LaddsError(rc, "bad elements")
-    return r, v
+    return _population.elements_to_state(a, e, inc, raan, argp, M)
 
 
 @dataclass

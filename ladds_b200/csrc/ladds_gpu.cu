@@ -1576,16 +1576,35 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   // current (cell-ordered) buffer
   const DevState S = c->snap;
   const int ni = (int)n;
-  CK(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
-  CK(cudaEventRecord(c->callStart, c->st));
+  // any failure once work is enqueued: nothing of this call may still run when
+  // it returns -- its copies into the caller's arrays and its kernels are
+  // drained on all three streams -- and the iteration is not counted (the device
+  // copy of the state is replaced by the next call's host state)
+  auto abortCall = [&](int rc) {
+    cudaStreamSynchronize(c->st2);
+    cudaStreamSynchronize(c->st3);
+    cudaStreamSynchronize(c->st);
+    cudaMemcpyAsync(c->dIter, &startIter, sizeof(int64_t), cudaMemcpyHostToDevice, c->st);
+    cudaStreamSynchronize(c->st);
+    c->orderValid = false;
+    return rc;
+  };
+#define CKS(call)                                                                                   \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      return abortCall(fail(c, LADDS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+  } while (0)
+  CKS(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
+  CKS(cudaEventRecord(c->callStart, c->st));
   if (n) {
     const int g = blocksFor(n, 256);
     k_unpermute_f64<<<g, 256, 0, c->st>>>(c->cur.aom, c->cur.tag, ni, S.aom);
     k_unpermute_f64<<<g, 256, 0, c->st>>>(c->cur.bc, c->cur.tag, ni, S.bc);
     k_unpermute_tag<<<g, 256, 0, c->st>>>(c->cur.tag, ni, S.tag);
   }
-  CK(enqueueEphemeris(c, 1));
-  if (scan) CK(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
+  CKS(enqueueEphemeris(c, 1));
+  if (scan) CKS(cudaMemsetAsync(c->rowCounts, 0, ((size_t)c->nRows + 1) * sizeof(uint32_t), c->st));
   // pageable arrays go through pinned staging, copied on all host threads
   // chunk by chunk (the CUDA driver's own staging of pageable copies is slower)
   bool stageIn[6] = {}, stageOut[6] = {}, anyIn = false, anyOut = false;
@@ -1628,18 +1647,18 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     const size_t len = std::min(per, n - lo);
     if (anyIn) hostCopy(pinIn, in, stageIn, lo, len);
     for (int a = 0; a < 6; ++a)
-      CK(cudaMemcpyAsync(sArr[a] + lo, src[a] + lo, len * sizeof(double), cudaMemcpyHostToDevice, c->st2));
-    CK(cudaEventRecord(c->evPipe[ch], c->st2));
-    CK(cudaStreamWaitEvent(c->st, c->evPipe[ch], 0));
+      CKS(cudaMemcpyAsync(sArr[a] + lo, src[a] + lo, len * sizeof(double), cudaMemcpyHostToDevice, c->st2));
+    CKS(cudaEventRecord(c->evPipe[ch], c->st2));
+    CKS(cudaStreamWaitEvent(c->st, c->evPipe[ch], 0));
     DevState Sc = S;
     Sc.x += lo; Sc.y += lo; Sc.z += lo; Sc.vx += lo; Sc.vy += lo; Sc.vz += lo;
     Sc.aom += lo; Sc.bc += lo; Sc.tag += lo;
     launchPropagate(c, Sc, (int)len, 1, 0, scan, c->keys0 + lo, c->scratchC + lo);
-    CK(cudaEventRecord(c->evPipe[kHostChunks + ch], c->st));
-    CK(cudaStreamWaitEvent(c->st3, c->evPipe[kHostChunks + ch], 0));
+    CKS(cudaEventRecord(c->evPipe[kHostChunks + ch], c->st));
+    CKS(cudaStreamWaitEvent(c->st3, c->evPipe[kHostChunks + ch], 0));
     for (int a = 0; a < 6; ++a)
-      CK(cudaMemcpyAsync(dstHost[a] + lo, sArr[a] + lo, len * sizeof(double), cudaMemcpyDeviceToHost, c->st3));
-    CK(cudaEventRecord(c->evPipe[2 * kHostChunks + ch], c->st3));
+      CKS(cudaMemcpyAsync(dstHost[a] + lo, sArr[a] + lo, len * sizeof(double), cudaMemcpyDeviceToHost, c->st3));
+    CKS(cudaEventRecord(c->evPipe[2 * kHostChunks + ch], c->st3));
     used = ch + 1;
   }
   k_advance<<<1, 32, 0, c->st>>>(c->dIter, 1);
@@ -1673,44 +1692,35 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     for (int a = 0; a < 6; ++a) k_permute_from_slots_f64<<<g, 256, 0, c->st>>>(sArr[a], c->cur.tag, ni, dst[a]);
   }
   if (used) {
-    CK(cudaEventRecord(c->evPipe[3 * kHostChunks], c->st3));
-    CK(cudaStreamWaitEvent(c->st, c->evPipe[3 * kHostChunks], 0));
+    CKS(cudaEventRecord(c->evPipe[3 * kHostChunks], c->st3));
+    CKS(cudaStreamWaitEvent(c->st, c->evPipe[3 * kHostChunks], 0));
   }
-  CK(cudaEventRecord(c->callEnd, c->st));
+  CKS(cudaEventRecord(c->callEnd, c->st));
   // staged outputs: each chunk leaves the pinned buffer as soon as it is there
   for (int ch = 0; ch < used && anyOut; ++ch) {
-    CK(cudaEventSynchronize(c->evPipe[2 * kHostChunks + ch]));
+    CKS(cudaEventSynchronize(c->evPipe[2 * kHostChunks + ch]));
     const size_t lo = (size_t)ch * per;
     hostCopy(outState, pinOut, stageOut, lo, std::min(per, n - lo));
   }
-  auto undo = [&](int rc) {
-    // the iteration is not counted; the device copy of the state is replaced by
-    // the next call's host state
-    cudaStreamSynchronize(c->st3);
-    cudaMemcpyAsync(c->dIter, &startIter, sizeof(int64_t), cudaMemcpyHostToDevice, c->st);
-    cudaStreamSynchronize(c->st);
-    c->orderValid = false;
-    return rc;
-  };
   unsigned long long cnt = 0;
   bool overflow = false;
   int rc = syncStatusAndGrow(c, &cnt, &overflow);
   collectTimes(c);
-  if (rc) return undo(rc);
+  if (rc) return abortCall(rc);
   int retries = 0;
   while (overflow) {  // the device buffers have grown: the scan alone runs again on the same state
-    if (++retries > 4) return undo(fail(c, LADDS_ERR_STATE, "device scan buffers kept overflowing"));
-    CK(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
+    if (++retries > 4) return abortCall(fail(c, LADDS_ERR_STATE, "device scan buffers kept overflowing"));
+    CKS(cudaMemsetAsync(c->dCount, 0, 2 * sizeof(unsigned long long), c->st));
     enqueueScanWith(c, c->st, sc, c->cutF, c->dIterBase, 0);
     rc = syncStatusAndGrow(c, &cnt, &overflow);
     collectTimes(c);
-    if (rc) return undo(rc);
+    if (rc) return abortCall(rc);
   }
-  CK(cudaStreamSynchronize(c->st3));
+  CKS(cudaStreamSynchronize(c->st3));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->callStart, c->callEnd);
   std::vector<ladds_pair> recs(cnt);
-  if (cnt) CK(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
+  if (cnt) CKS(cudaMemcpy(recs.data(), c->dPairs, cnt * sizeof(ladds_pair), cudaMemcpyDeviceToHost));
   std::sort(recs.begin(), recs.end(), pairLess);
   c->hostIter += 1;
   if (scan) c->orderValid = true;
@@ -1733,6 +1743,7 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   }
   if (!recs.empty()) std::memcpy(out, recs.data(), recs.size() * sizeof(ladds_pair));
   return LADDS_OK;
+#undef CKS
 }
 
 int ladds_gpu_pending_records(ladds_gpu_ctx *c, ladds_pair *out, size_t cap, size_t *nOut) {
@@ -2466,12 +2477,34 @@ int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, 
     naMessage(errMsg, errMsgCap, text);
     return LADDS_ERR_TOO_LARGE;
   }
+  // an error that earlier work left in this thread's CUDA state is not this
+  // call's: report it without clearing it
+  if (const cudaError_t pending = cudaPeekAtLastError(); pending != cudaSuccess) {
+    char text[200];
+    std::snprintf(text, sizeof(text), "a CUDA error of earlier work is pending (not cleared): %s",
+                  cudaGetErrorString(pending));
+    naMessage(errMsg, errMsgCap, text);
+    return LADDS_ERR_CUDA;
+  }
   DeviceGuard guard(device);
   if (guard.status != cudaSuccess) {
     cudaGetLastError();
     naMessage(errMsg, errMsgCap, cudaGetErrorString(guard.status));
     return guard.status == cudaErrorInvalidDevice || guard.status == cudaErrorNoDevice ? LADDS_ERR_NO_DEVICE
                                                                                         : LADDS_ERR_CUDA;
+  }
+  // the call waits for its stream and reads a status word back: it cannot be
+  // part of a stream capture
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  if (const cudaError_t ce = cudaStreamIsCapturing(s, &capturing); ce != cudaSuccess) {
+    cudaGetLastError();
+    naMessage(errMsg, errMsgCap, cudaGetErrorString(ce));
+    return LADDS_ERR_CUDA;
+  }
+  if (capturing != cudaStreamCaptureStatusNone) {
+    naMessage(errMsg, errMsgCap, "invalid argument: the stream is capturing; this call synchronises its stream");
+    return LADDS_ERR_INVALID_ARG;
   }
   NaDevice &d = g_naDevice[device];
   {
@@ -2490,7 +2523,6 @@ int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, 
       d.scratch = ptr;
     }
   }
-  cudaStream_t s = (cudaStream_t)stream;
   const uint32_t nx = (uint32_t)dims[0], nRows = (uint32_t)nRows64;
   auto *rec = reinterpret_cast<unsigned long long *>(d.scratch + kNaRec);
   auto *src = reinterpret_cast<uint32_t *>(d.scratch + kNaSrc);
@@ -2503,34 +2535,56 @@ int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, 
   auto *s1 = reinterpret_cast<uint32_t *>(d.scratch + kNaScan);
   uint32_t *s1x = s1 + kNaScanBlocks + 1, *s2 = s1x + kNaScanBlocks + 1;
 
-  cudaMemsetAsync(rowCount, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), s);
-  cudaMemsetAsync(longCount, 0, 2 * sizeof(uint32_t), s);  // longCount and status
-  if (n) {
+  // every enqueue is checked where it is made; on a failure the stream is
+  // drained before returning, so that no copy of this call is still running
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t r) {
+    if (e == cudaSuccess && r != cudaSuccess) e = r;
+    return e == cudaSuccess;
+  };
+  ok(cudaMemsetAsync(rowCount, 0, 2 * ((size_t)nRows + 1) * sizeof(uint32_t), s));
+  ok(cudaMemsetAsync(longCount, 0, 2 * sizeof(uint32_t), s));  // longCount and status
+  if (e == cudaSuccess && n) {
     const int gridN = blocksFor(n, kBucketThreads);
     k_na_count<<<gridN, kBucketThreads, 0, s>>>(keys, (int)n, nx, nRows, rowCount, status);
+    ok(cudaGetLastError());
   }
   const size_t count = (size_t)nRows + 1;
   const int nb1 = blocksFor(count, kScanBlock);
-  k_scan_blocks<<<nb1, kScanBlock, 0, s>>>(rowCount, (int)count, rowStartS, s1);
-  if (nb1 > 1) {
-    k_scan_blocks<<<1, kScanBlock, 0, s>>>(s1, nb1, s1x, s2);
-    k_scan_add<<<nb1, kScanBlock, 0, s>>>(rowStartS, (int)count, s1x);
+  if (e == cudaSuccess) {
+    k_scan_blocks<<<nb1, kScanBlock, 0, s>>>(rowCount, (int)count, rowStartS, s1);
+    ok(cudaGetLastError());
   }
-  if (n) {
+  if (e == cudaSuccess && nb1 > 1) {
+    k_scan_blocks<<<1, kScanBlock, 0, s>>>(s1, nb1, s1x, s2);
+    if (ok(cudaGetLastError())) {
+      k_scan_add<<<nb1, kScanBlock, 0, s>>>(rowStartS, (int)count, s1x);
+      ok(cudaGetLastError());
+    }
+  }
+  if (e == cudaSuccess && n) {
     const int gridN = blocksFor(n, kBucketThreads);
     k_na_scatter<<<gridN, kBucketThreads, 0, s>>>(keys, (int)n, nx, nRows, rowStartS, rowCursor, rec, src, status);
-    const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 64 * d.sms);
-    k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, s>>>(rowStartS, nRows, nx, rec, src, sortedKeys, order,
-                                                               longRows, longCount, nullptr);
-    k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(
-        rowStartS, nx, rec, src, sortedKeys, order, longRows, longCount, nullptr, DenseBin{nullptr, nullptr, 0, 0});
+    if (ok(cudaGetLastError())) {
+      const int smallBlocks = std::min(blocksFor((size_t)nRows * 32, kBucketThreads), 64 * d.sms);
+      k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, s>>>(rowStartS, nRows, nx, rec, src, sortedKeys, order,
+                                                                 longRows, longCount, nullptr);
+    }
+    if (ok(cudaGetLastError())) {
+      k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(
+          rowStartS, nx, rec, src, sortedKeys, order, longRows, longCount, nullptr,
+          DenseBin{nullptr, nullptr, 0, 0});
+      ok(cudaGetLastError());
+    }
   }
-  if (rowStart) cudaMemcpyAsync(rowStart, rowStartS, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && rowStart)
+    ok(cudaMemcpyAsync(rowStart, rowStartS, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   unsigned hostStatus = 0;
-  cudaMemcpyAsync(&hostStatus, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamSynchronize(s);
-  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) ok(cudaMemcpyAsync(&hostStatus, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  const cudaError_t es = cudaStreamSynchronize(s);  // also on a failure: nothing of this call left running
+  ok(es);
   if (e != cudaSuccess) {
+    cudaGetLastError();
     naMessage(errMsg, errMsgCap, cudaGetErrorString(e));
     return LADDS_ERR_CUDA;
   }

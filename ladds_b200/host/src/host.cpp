@@ -432,7 +432,10 @@ size_t HotPathLoop::run(size_t n) {
   if (!gpu_.mirrors(container_)) gpu_.upload(container_);
   size_t totalCollisions = 0;
   for (size_t done = 0; done < n; ++done, ++iteration_) {
-    if (iterationsSinceLastCollision_ == 100) gpu_.check(ladds_gpu_clear_parents(gpu_.handle()));
+    if (iterationsSinceLastCollision_ == 100) {  // Simulation::removeParticleSpawnProtection, on both copies
+      gpu_.check(ladds_gpu_clear_parents(gpu_.handle()));
+      for (auto &p : container_) p.setParentIdentifier(std::numeric_limits<size_t>::max());
+    }
     gpu_.check(ladds_gpu_integrate(gpu_.handle(), 1));
     // burn-ups: removed on the device and, by id, from the container
     const size_t before = gpu_.deviceSize();

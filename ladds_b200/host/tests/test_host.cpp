@@ -173,6 +173,25 @@ static void gpuTests() {
     CHECK(!c.empty() && c.front().getID() == 1);
     CHECK(gpu.deviceSize() == 1);
   }
+  // Spawn protection (Simulation.cpp:291-293, :401, :438, :470-473): two
+  // fragments of one breakup, 0.5 m apart on the same orbit, are skipped while
+  // they share a parent; the 100th collision-free iteration resets every
+  // parent id before it integrates, and the pair collides in that iteration.
+  {
+    auto cfg = ladds::ConfigReader::fromString(kSimConfig);
+    ladds::GpuContext gpu(ladds::GpuContext::configFrom(cfg));
+    const double vc = std::sqrt(398600.4418 / 7000.);
+    ladds::Container c;
+    c.push_back(mk({7000., 0., 0.}, {0., vc, 0.}, 10, AS::passive, 1., 7));
+    c.push_back(mk({7000., 0.0005, 0.}, {0., vc, 1e-7}, 11, AS::passive, 1., 7));
+    c.push_back(mk({-7000., 0., 0.}, {0., -vc, 0.}, 12, AS::passive, 1.));  // far away, no parent
+    ladds::HotPathLoop loop(cfg, c, gpu);
+    CHECK(loop.run(100) == 0);  // iterations 0..99: same parent, skipped (CollisionFunctor.cpp:64-67)
+    CHECK(c[0].getParentIdentifier() == 7 && c[1].getParentIdentifier() == 7);
+    CHECK(loop.run(1) == 1);  // iteration 100: protection removed, the pair is a collision
+    CHECK(c[0].getParentIdentifier() == kNoParent && c[1].getParentIdentifier() == kNoParent);
+    CHECK(loop.run(3) == 3);  // and stays one
+  }
   // Integrator: host-owned mode writes the state back after every step
   {
     auto cfg = ladds::ConfigReader::fromString(kSimConfig);

@@ -1,9 +1,9 @@
 """Regenerates the golden fixtures in this directory from the LADDS source tree.
 
-Run in a container where the reference tree is mounted (default location
-``/root/reference``; override with ``LADDS_REFERENCE``)::
+Run with the path of an esa/LADDS source tree, given as ``--reference DIR``
+or in the environment variable ``LADDS_REFERENCE``::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference path/to/LADDS
 
 It reads, as text:
   * tests/testladds/CollisionFunctorTest.cpp -- the parametrised
@@ -16,11 +16,13 @@ the tests read; the reference tree is never read at test time.
 """
 from __future__ import annotations
 
+import argparse
 import json
 import os
 import re
+import sys
 
-REF = os.environ.get("LADDS_REFERENCE", "/root/reference")
+REF = None  # the LADDS source tree, set by main()
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -63,6 +65,16 @@ def two_body_fixture():
 
 
 def main():
+    global REF
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=os.environ.get("LADDS_REFERENCE"),
+                    help="esa/LADDS source tree (default: $LADDS_REFERENCE)")
+    args = ap.parse_args()
+    if not args.reference or not os.path.isfile(
+            os.path.join(args.reference, "tests", "testladds", "CollisionFunctorTest.cpp")):
+        sys.exit("make_golden.py: give the esa/LADDS source tree with --reference DIR or LADDS_REFERENCE "
+                 f"(got {args.reference!r})")
+    REF = args.reference
     with open(os.path.join(OUT, "interpolation_cases.json"), "w") as f:
         json.dump(interpolation_cases(), f, indent=1)
     with open(os.path.join(OUT, "two_body_10s.json"), "w") as f:

@@ -48,5 +48,34 @@ def test_reference_arm_on_population_file(tmp_path):
     assert "pop.bin" in d["config"]["workload"]
 
 
+def test_reference_arm_loads_no_gpu_code_and_prints_the_gpu_arms_config():
+    """The reference arm maps none of the package's GPU libraries (its
+    population comes from the host-only generator), and its config dict is the
+    one the GPU arm prints (bench.bench_config)."""
+    code = (
+        "import json, runpy, sys, io, contextlib\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '3', '--n-objects', '2000',"
+        " '--reference-budget', '1']\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf):\n"
+        f"    runpy.run_path({os.path.join(ROOT, 'bench.py')!r}, run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'line': buf.getvalue(), 'gpu_lib': 'libladds_gpu' in maps,"
+        " 'peaks_lib': 'libladds_peaks' in maps}))\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert not out["gpu_lib"] and not out["peaks_lib"]
+    d = json.loads(out["line"].strip().splitlines()[-1])
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class A:
+        population = None
+        n_objects = 2000
+
+    assert d["config"] == bench.bench_config(A, 2000)
+
+
 def test_reference_arm_other_ranks_are_silent():
     assert run_bench("--steps", "1", "--warmup", "3", env={"WORLD_SIZE": "2", "RANK": "1", "LOCAL_RANK": "1"}) == []

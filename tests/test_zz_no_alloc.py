@@ -153,3 +153,47 @@ def test_noalloc_sort_rejects_sizes_beyond_its_maximum(env):
     ref = np.lexsort((np.arange(1000), keys))
     assert np.array_equal(order, ref.astype(np.uint32)) and np.array_equal(skeys, keys[ref])
     assert np.array_equal(row_start.astype(np.int64), np.searchsorted(keys[ref] // 4, np.arange(17)))
+
+
+def test_noalloc_sort_empty_input_and_no_row_table(env):
+    """n = 0 fills the row table with zeros; a NULL row table is allowed."""
+    torch, capi = env
+    rc, msg, skeys, order, row_start = noalloc_sort(torch, capi, np.zeros(0, np.uint32), (4, 4, 4))
+    assert rc == capi.OK, msg
+    assert len(skeys) == 0 and len(order) == 0 and np.all(row_start == 0)
+    keys = np.random.default_rng(11).integers(0, 64, size=500).astype(np.uint32)
+    L = capi.lib()
+    dkeys = torch.from_numpy(keys.view(np.int32)).cuda()
+    out_keys = torch.empty(500, dtype=torch.int32, device="cuda")
+    out_order = torch.empty(500, dtype=torch.int32, device="cuda")
+    msg = C.create_string_buffer(256)
+    rc = L.ladds_gpu_cell_sort_noalloc(0, C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                       C.c_void_p(dkeys.data_ptr()), 500, C.byref((C.c_int32 * 3)(4, 4, 4)),
+                                       C.c_void_p(out_keys.data_ptr()), C.c_void_p(out_order.data_ptr()), None, msg,
+                                       256)
+    assert rc == capi.OK, msg.value
+    ref = np.lexsort((np.arange(500), keys))
+    assert np.array_equal(out_order.cpu().numpy().view(np.uint32), ref.astype(np.uint32))
+
+
+def test_noalloc_sort_refuses_a_capturing_stream(env):
+    """The call synchronises its stream, so a capturing stream is refused
+    before anything is enqueued (the capture stays valid)."""
+    torch, capi = env
+    L = capi.lib()
+    keys = torch.zeros(16, dtype=torch.int32, device="cuda")
+    out_keys = torch.empty(16, dtype=torch.int32, device="cuda")
+    out_order = torch.empty(16, dtype=torch.int32, device="cuda")
+    msg = C.create_string_buffer(256)
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        rc = L.ladds_gpu_cell_sort_noalloc(0, C.c_void_p(side.cuda_stream), C.c_void_p(keys.data_ptr()), 16,
+                                           C.byref((C.c_int32 * 3)(4, 4, 4)), C.c_void_p(out_keys.data_ptr()),
+                                           C.c_void_p(out_order.data_ptr()), None, msg, 256)
+        out_keys.add_(1)  # the capture still records work after the refusal
+    assert rc == capi.ERR_INVALID_ARG and "capturing" in msg.value.decode()
+    g.replay()
+    torch.cuda.synchronize()
+    del g
