@@ -369,28 +369,51 @@ def objects_at_steps(capi, cfg, pop, wanted):
     return out
 
 
+LIST_BITS = 1 | 2 | 4  # collision, evasion, conjunction
+NEAR_BITS = 8 | 16 | 32 | 64  # near bands of those thresholds and of the cutoff gate
+
+
 def classify_differences(capi, cfgs, pop, recs, dt):
-    """Each record that only one precision lists: the pair's own split-vs-FP64
-    difference at that step (states re-run to that step in both precisions)
-    against its margin to the threshold it crosses.  A record is explained when
-    the threshold or the cutoff lies within the pair's drift bound
-    |dr_A| + |dr_B| + dt (|dv_A| + |dv_B|) of its distance."""
-    key = lambda r: (int(r["step"]), int(r["idA"]), int(r["idB"]), int(r["flags"]) & 7)
-    ka = {key(r): r for r in recs["split"]}
-    kb = {key(r): r for r in recs["fp64"]}
-    diff = [(k, ka.get(k, kb.get(k))) for k in sorted(set(ka) ^ set(kb))]
+    """The conjunction sets (records with a collision, evasion or conjunction
+    bit) of the two precisions, pair by pair.  Records that carry only a
+    near-band flag (listed separately, not part of the set) are counted apart.
+    A pair whose list bits differ is near-flagged when either run flags it in
+    the near band of a threshold or of the cutoff gate; otherwise its
+    split-vs-FP64 difference at that step (states re-run to that step in both
+    precisions) is set against its margin to the threshold it crosses: the
+    difference is explained when the threshold (or the cutoff) lies within the
+    pair's drift bound |dr_A| + |dr_B| + dt (|dv_A| + |dv_B|) of its distance."""
+    key = lambda r: (int(r["step"]), int(r["idA"]), int(r["idB"]))
+    ta = {key(r): r for r in recs["split"]}
+    tb = {key(r): r for r in recs["fp64"]}
+    flags = lambda t, k: int(t[k]["flags"]) if k in t else 0
+    in_set = {name: sum(1 for r in t.values() if int(r["flags"]) & LIST_BITS) for name, t in (("split", ta),
+                                                                                            ("fp64", tb))}
+    near_only = sum(1 for k in set(ta) ^ set(tb) if not (flags(ta, k) | flags(tb, k)) & LIST_BITS)
+    diff, near = [], 0
+    for k in sorted(set(ta) | set(tb)):
+        fa, fb = flags(ta, k), flags(tb, k)
+        if (fa & LIST_BITS) == (fb & LIST_BITS):
+            continue
+        if (fa | fb) & NEAR_BITS:
+            near += 1
+            continue
+        diff.append((k, ta.get(k, tb.get(k)), "split" if fa & LIST_BITS else "fp64"))
+    out = {"set_split": in_set["split"], "set_fp64": in_set["fp64"], "set_differences": near + len(diff),
+           "near_flagged": near, "not_near_flagged": len(diff), "near_band_only_records_differing": near_only}
     if not diff:
-        return {"records_only_in_one": 0, "explained": 0}
+        out["explained_by_drift"] = 0
+        return out
     wanted = set()
-    for _, r in diff:
+    for _, r, _ in diff:
         wanted.add((int(r["step"]), int(r["slotA"])))
         wanted.add((int(r["step"]), int(r["slotB"])))
     st = {name: objects_at_steps(capi, cfgs[name], pop, wanted) for name in ("split", "fp64")}
     cfg = cfgs["fp64"]
     rows = []
-    for k, r in diff:
+    for k, r, where in diff:
         s_, a, b = int(r["step"]), int(r["slotA"]), int(r["slotB"])
-        (ra, va, rad_a, act_a), (rb, vb, rad_b, act_b) = st["split"][(s_, a)], st["split"][(s_, b)]
+        (ra, va, rad_a, _), (rb, vb, rad_b, _) = st["split"][(s_, a)], st["split"][(s_, b)]
         (ra2, va2, _, _), (rb2, vb2, _, _) = st["fp64"][(s_, a)], st["fp64"][(s_, b)]
         bound = (np.linalg.norm(ra - ra2) + np.linalg.norm(rb - rb2)
                  + dt * (np.linalg.norm(va - va2) + np.linalg.norm(vb - vb2)))
@@ -398,19 +421,15 @@ def classify_differences(capi, cfgs, pop, recs, dt):
         d2, dl2 = closest_approach(ra2, va2, rb2, vb2, dt)
         thr = [cfg.conjunctionThreshold, cfg.evasionCutoff,
                (rad_a + rad_b) * cfg.collisionDistanceFactor / 1000.0]
-        margins = [(abs(dl1 - t), t) for t in thr] + [(abs(d1 - cfg.cutoff), cfg.cutoff)]
-        m, t = min(margins)
-        rows.append({"step": s_, "in": "split" if k in ka else "fp64", "margin_km": float(m), "threshold_km": t,
-                     "bound_km": float(bound), "dl_split_km": float(dl1), "dl_fp64_km": float(dl2),
-                     "straddles": bool(min(dl1, dl2) - 1e-12 <= t <= max(dl1, dl2) + 1e-12
-                                       or min(d1, d2) - 1e-12 <= t <= max(d1, d2) + 1e-12)})
+        m, t = min([(abs(dl1 - t_), t_) for t_ in thr] + [(abs(d1 - cfg.cutoff), cfg.cutoff)])
+        rows.append({"step": s_, "in": where, "margin_km": float(m), "threshold_km": t, "bound_km": float(bound),
+                     "dl_split_km": float(dl1), "dl_fp64_km": float(dl2)})
     explained = [x for x in rows if x["margin_km"] <= x["bound_km"] * (1 + 1e-6) + 1e-12]
-    return {"records_only_in_one": len(rows), "explained": len(explained),
-            "straddling_a_threshold": sum(x["straddles"] for x in rows),
-            "max_margin_m": max(x["margin_km"] for x in rows) * 1e3,
-            "max_margin_rel": max(x["margin_km"] / x["threshold_km"] for x in rows),
-            "max_pair_drift_bound_m": max(x["bound_km"] for x in rows) * 1e3,
-            "first_step": min(x["step"] for x in rows), "examples": rows[:3]}
+    out.update({"explained_by_drift": len(explained),
+                "max_margin_m": max(x["margin_km"] for x in rows) * 1e3,
+                "max_margin_rel": max(x["margin_km"] / x["threshold_km"] for x in rows),
+                "max_pair_drift_bound_m": max(x["bound_km"] for x in rows) * 1e3, "examples": rows[:3]})
+    return out
 
 
 def drift_leg(capi, device, pop, steps, cfg_kw=None):
@@ -443,37 +462,41 @@ def drift_leg(capi, device, pop, steps, cfg_kw=None):
     return out
 
 
-def breakup_leg(capi, device, pop, iterations, cfg_kw):
-    """Config 4 form: every iteration one ladds_gpu_step(1), then the NASA
-    breakup model on the host for the iteration's collision records, the
-    fragments appended on the device (BreakupWrapper.cpp:13-45,
-    Simulation.cpp:610-633).  Also the expected collision rate of the
-    conjunction records, sum of ((r_A + r_B) / 0.1 km)^2 over them (the
-    fraction of a uniform-in-area miss distribution inside the collision
-    radius)."""
+def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
+    """Config 4 form, the reference loop (Simulation.cpp:287-415) per
+    iteration: integrate; burn-ups below min_altitude removed (:302); particles
+    leaving the container (outside the box, or a non-finite state) removed
+    (:314, :381-387); the conjunction scan; the NASA breakup model on the host
+    for every collision, its fragments appended on the device
+    (BreakupWrapper.cpp:13-45, Simulation.cpp:610-633).  Also the expected
+    collision count of the conjunction records, sum of ((r_A + r_B) / 0.1 km)^2
+    over them (the fraction of a uniform-in-area miss distribution inside the
+    collision radius)."""
     cfg = capi.default_config(componentMask=capi.PROP_ALL, precision=capi.PRECISION_SPLIT, device=device,
                               pairCapacity=1 << 18, **cfg_kw)
     bcfg = capi.BreakupConfig(0.05, 1, 2.2)
-    radius = pop["radius"]
     n = len(pop["x"])
     next_id = int(np.max(pop["id"])) + 1 if n else 0
-    tot = dict(breakups=0, fragments=0, collisions=0, conjunctions=0)
+    tot = dict(breakups=0, fragments=0, collisions=0, conjunctions=0, burnups=0, escaped=0, nonfinite_steps=0)
     expected = 0.0
     t0 = time.perf_counter()
-    dev_ms = 0.0
     with capi.Context(cfg) as ctx:
         ctx.upload(pop)
         for it in range(iterations):
-            r = ctx.step(1)
-            dev_ms += r.stats.deviceMs
-            rec = r.records
-            tot["collisions"] += int(r.stats.collisions)
+            if not ctx.integrate(1, allow_nonfinite=True):
+                tot["nonfinite_steps"] += 1
+            tot["burnups"] += len(ctx.remove_below(min_altitude))
+            tot["escaped"] += len(ctx.remove_escaping())
+            rec = ctx.conjunctions(cfg.deltaT)
+            col = rec[(rec["flags"] & capi.PAIR_COLLISION) != 0]
             conj = rec[(rec["flags"] & capi.PAIR_CONJUNCTION) != 0]
+            tot["collisions"] += len(col)
             tot["conjunctions"] += len(conj)
-            sa, sb = conj["slotA"].astype(np.int64), conj["slotB"].astype(np.int64)
-            ok = (sa < n) & (sb < n)  # fragments (slots >= n) carry their own radii; the original ones suffice here
-            expected += float(np.sum(((radius[sa[ok]] + radius[sb[ok]]) * 1e-3 / 0.1) ** 2))
-            if r.stats.collisions:
+            if len(conj):
+                objs = ctx.get_objects(np.concatenate([conj["slotA"], conj["slotB"]]))
+                ra, rb = objs["radius"][: len(conj)], objs["radius"][len(conj):]
+                expected += float(np.sum(((ra + rb) * cfg.collisionDistanceFactor * 1e-3 / 0.1) ** 2))
+            if len(col):
                 nb, nf, next_id = ctx.breakup(rec, bcfg, 1000 + it, next_id)
                 tot["breakups"] += nb
                 tot["fragments"] += nf
@@ -481,16 +504,53 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw):
     wall = time.perf_counter() - t0
     return {"iterations": iterations, "hours": iterations * cfg.deltaT / 3600.0, **tot,
             "expected_collisions_from_conjunctions": expected, "objects_after": size,
-            "ms_per_iteration_wall": wall * 1e3 / iterations, "ms_per_iteration_device": dev_ms / iterations}
+            "ms_per_iteration_wall": wall * 1e3 / iterations}
 
 
 # ---------------------------------------------------------- adjoint leg
+def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6):
+    """Finite-difference check of directional derivatives gd (one per pair)
+    from the losses f0 at x and fm[k] at x + c_k eps d, c = (1, -1, 1/2, -1/2),
+    with the argmin steps step0 / stepm[k] of each evaluation.
+
+    The loss is a minimum over steps (and, inside a step, over the clamped
+    closest-approach time), so it has kinks where two branches tie; the
+    gradient is the derivative of the branch active at x.  Per pair and per
+    side: a side whose two points keep the argmin step gives a one-sided
+    Richardson extrapolation (second order, from h and h / 2); if both sides
+    keep it and agree, the central Richardson value is used; if they disagree
+    the stencil straddles a kink inside the step (the clamp of the time) and
+    the side that agrees with the active branch is taken; pairs where neither
+    side keeps the argmin are unresolved at this h.  Returns the per-pair
+    relative errors and the counts of each class."""
+    keep = stepm == step0[None, :]
+    keep_p, keep_m = keep[0] & keep[2], keep[1] & keep[3]
+    fwd = (4.0 * (fm[2] - f0) / (0.5 * eps) - (fm[0] - f0) / eps) / 3.0
+    bwd = (4.0 * (f0 - fm[3]) / (0.5 * eps) - (f0 - fm[1]) / eps) / 3.0
+    cen = (4.0 * (fm[2] - fm[3]) / eps - (fm[0] - fm[1]) / (2 * eps)) / 3.0
+    scale = np.maximum(np.abs(cen), 1e-300)
+    both = keep_p & keep_m
+    agree = both & (np.abs(fwd - bwd) <= tol * scale)
+    rel = np.full(len(gd), np.inf)
+    err = lambda ref: np.abs(gd - ref) / np.maximum(np.abs(ref), 1e-300)
+    rel[agree] = err(cen)[agree]
+    kink = both & ~agree
+    rel[kink] = np.minimum(err(fwd), err(bwd))[kink]
+    only_p, only_m = keep_p & ~keep_m, keep_m & ~keep_p
+    rel[only_p] = err(fwd)[only_p]
+    rel[only_m] = err(bwd)[only_m]
+    unresolved = ~keep_p & ~keep_m
+    counts = {"central": int(agree.sum()), "kink_inside_step": int(kink.sum()), "forward_only": int(only_p.sum()),
+              "backward_only": int(only_m.sum()), "unresolved": int(unresolved.sum())}
+    return rel, counts
+
+
 def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
     """Differentiation workload: 4096 pairs, 1080 FP64 steps of the full force
     set, checkpoints every 64 steps.  Device times of the forward sweep (loss +
     checkpoints) and of the backward sweep (segment recompute + reverse sweep),
-    and a directional central-difference check of every pair's gradient
-    (Richardson-extrapolated from eps and eps / 2, eps = 1e-6 |x|)."""
+    and a directional finite-difference check of every pair's gradient at
+    h = 1e-6 |x| (and h / 2; fd_classify)."""
     with capi.Context(capi.default_config(componentMask=capi.PROP_ALL, device=device)) as ctx:
         pairs, _ = ctx.adjoint_make_pairs(77, n_pairs, steps)
         ctx.adjoint_forward(pairs, steps, ck)
@@ -512,26 +572,21 @@ def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
             q["rA"], q["vA"], q["rB"], q["vB"] = r[:, 0:3], r[:, 3:6], r[:, 6:9], r[:, 9:12]
             batch.append(q)
         _, miss, stepP, _ = ctx.adjoint_forward(np.concatenate(batch), steps, ck)
-        step0 = ctx.adjoint_forward(pairs, steps, ck)[2]
-    miss = miss.reshape(4, n_pairs)
-    smooth = np.all(stepP.reshape(4, n_pairs) == step0[None, :], axis=0)  # the stencil keeps the argmin
-    fd1 = (miss[0] - miss[1]) / (2 * eps)
-    fd2 = (miss[2] - miss[3]) / eps
-    rich = (4.0 * fd2 - fd1) / 3.0
+        _, miss0, step0, _ = ctx.adjoint_forward(pairs, steps, ck)
     gd = np.sum(dx * d, axis=1)
-    rel = (np.abs(gd - rich) / np.abs(rich))[smooth]
-    rel1 = (np.abs(gd - fd1) / np.abs(fd1))[smooth]
+    rel, counts = fd_classify(gd, miss0, miss.reshape(4, n_pairs), step0, stepP.reshape(4, n_pairs), eps)
+    fin = rel[np.isfinite(rel)]
     f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    fd = {"direction": "random per pair, 12 state components, relative scaling", "h": "1e-6 |x| and h/2",
+          "pairs": n_pairs, **counts,
+          "meets_1e-6": int(np.sum(rel <= 1e-6)), "meets_1e-6_frac": float(np.mean(rel <= 1e-6)),
+          "rel_err_median": float(np.median(fin)) if len(fin) else None,
+          "rel_err_p99": float(np.quantile(fin, 0.99)) if len(fin) else None}
     return {"pairs": n_pairs, "steps": steps, "checkpoint_every": ck, "forward_ms": f_ms, "backward_ms": b_ms,
             "backward_over_forward": b_ms / f_ms, "forward_plus_backward_over_forward": (f_ms + b_ms) / f_ms,
-            "fd_check": {"direction": "random per pair, 12 state components, relative scaling",
-                         "pairs_checked": int(np.sum(smooth)),
-                         "pairs_skipped_argmin_switch": int(np.sum(~smooth)),
-                         "nonfinite": int(np.sum(~np.isfinite(rel))),
-                         "richardson_rel_err_median": float(np.nanmedian(rel)),
-                         "richardson_rel_err_p99": float(np.nanquantile(rel, 0.99)),
-                         "central_h1e-6_rel_err_median": float(np.nanmedian(rel1)),
-                         "central_h1e-6_rel_err_p99": float(np.nanquantile(rel1, 0.99))}}
+            "fd_check": fd,
+            "fd_summary": {"meets_1e-6_frac": fd["meets_1e-6_frac"], "unresolved": counts["unresolved"],
+                           "median": fd["rel_err_median"]}}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -778,15 +833,15 @@ def main():
         "propagate_fp64_over_split": fp64_per["propagate"] / max(per["propagate"], 1e-12),
         "mixed_over_fp64_bound_propagation_free": sum(fp64_per.values()) / shared_ms,
         "drift": {k: ({"steps": v["steps"], "rms_m": round(v["rms_m"], 5), "max_m": round(v["max_m"], 4),
-                       "records": [v["records_split"], v["records_fp64"]],
-                       "only_in_one": v["differences"]["records_only_in_one"],
-                       "explained": v["differences"]["explained"],
-                       "max_margin_m": v["differences"].get("max_margin_m")} if "error" not in v else v)
+                       "set": [v["differences"]["set_split"], v["differences"]["set_fp64"]],
+                       "set_differences": v["differences"]["set_differences"],
+                       "near_flagged": v["differences"]["near_flagged"],
+                       "explained_by_drift": v["differences"]["explained_by_drift"]} if "error" not in v else v)
                   for k, v in drift.items()},
         "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
         "adjoint_fd": (adjoint or {}).get("fd_summary"),
-        "breakups_8e6": ({k: breakups[k] for k in ("iterations", "collisions", "breakups", "fragments",
-                                                    "expected_collisions_from_conjunctions")}
+        "breakups_8e6": ({k: breakups[k] for k in ("iterations", "collisions", "breakups", "fragments", "burnups",
+                                                    "escaped", "expected_collisions_from_conjunctions")}
                          if breakups and "error" not in breakups else breakups),
         "value_over_cpu_baseline": value / cpu["value"] if cpu and cpu.get("value") else None,
     }

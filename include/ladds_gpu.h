@@ -189,7 +189,10 @@ int ladds_gpu_iteration(const ladds_gpu_ctx *ctx, int64_t *iteration);
 int ladds_gpu_set_iteration(ladds_gpu_ctx *ctx, int64_t iteration);
 
 /* Replaces YoshidaIntegrator::integrate(false) (Simulation.cpp:297): `steps`
- * Yoshida-4 steps of every particle.  Advances the iteration counter. */
+ * Yoshida-4 steps of every particle.  Advances the iteration counter.  A
+ * position or velocity that became non-finite returns LADDS_ERR_NONFINITE with
+ * the steps taken and the state kept (ladds_gpu_remove_escaping drops such
+ * particles, as the reference's container update does). */
 int ladds_gpu_integrate(ladds_gpu_ctx *ctx, int steps);
 
 /* Replaces collisionDetection() (Simulation.cpp:211-222) on the current
@@ -243,6 +246,16 @@ int ladds_gpu_pending_records(ladds_gpu_ctx *ctx, ladds_pair *out, size_t cap, s
  * removedIds (may be NULL) receives up to cap ids of removed particles. */
 int ladds_gpu_remove_below(ladds_gpu_ctx *ctx, double minAltitude, size_t *nRemoved, uint64_t *removedIds,
                            size_t cap);
+/* Deletes the particles that leave the container after an integration: a
+ * position or velocity that is not finite, or a position outside the
+ * configuration's [boxMin, boxMax] (AutoPas::updateContainer returns them as
+ * leaving particles, Simulation.cpp:314, and the reference reports them as
+ * escaping and drops them, :381-387).  An integration that produced non-finite
+ * states returns LADDS_ERR_NONFINITE from ladds_gpu_integrate with the state
+ * kept; this call then removes those particles.  Survivors keep their relative
+ * slot order and are renumbered 0..n'-1; removedIds (may be NULL) receives up
+ * to cap ids of removed particles. */
+int ladds_gpu_remove_escaping(ladds_gpu_ctx *ctx, size_t *nRemoved, uint64_t *removedIds, size_t cap);
 /* Marks particles (by slot) as deleted: they are skipped by propagation and
  * scans (the dummy ownership state of Simulation.cpp:368-371). */
 int ladds_gpu_mark_deleted(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t n);

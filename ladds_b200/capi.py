@@ -79,7 +79,8 @@ EXPORTED = [
     "ladds_gpu_last_error", "ladds_gpu_upload", "ladds_gpu_append", "ladds_gpu_download", "ladds_gpu_set_state",
     "ladds_gpu_get_state", "ladds_gpu_size", "ladds_gpu_iteration", "ladds_gpu_set_iteration",
     "ladds_gpu_integrate", "ladds_gpu_conjunctions", "ladds_gpu_step", "ladds_gpu_remove_below",
-    "ladds_gpu_mark_deleted", "ladds_gpu_clear_parents", "ladds_gpu_cell_order", "ladds_gpu_grid",
+    "ladds_gpu_mark_deleted", "ladds_gpu_remove_escaping", "ladds_gpu_clear_parents", "ladds_gpu_cell_order",
+    "ladds_gpu_grid",
     "ladds_gpu_phase_times", "ladds_gpu_set_profiling", "ladds_population_generate", "ladds_elements_to_state",
     "ladds_gpu_functor_pairs", "ladds_gpu_scan", "ladds_gpu_cell_sort_noalloc", "ladds_gpu_adjoint_forward",
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
@@ -160,6 +161,7 @@ def lib():
                                       C.POINTER(StepStats)]
     L.ladds_gpu_pending_records.argtypes = [vp, vp, sz, C.POINTER(sz)]
     L.ladds_gpu_remove_below.argtypes = [vp, C.c_double, C.POINTER(sz), vp, sz]
+    L.ladds_gpu_remove_escaping.argtypes = [vp, C.POINTER(sz), vp, sz]
     L.ladds_gpu_mark_deleted.argtypes = [vp, vp, sz]
     L.ladds_gpu_clear_parents.argtypes = [vp]
     L.ladds_gpu_cell_order.argtypes = [vp, sz, C.POINTER(sz), vp, vp]
@@ -318,8 +320,14 @@ class Context:
         self._check(self._L.ladds_gpu_get_state(self._h, n, *[_p(a) for a in arrs]))
         return arrs
 
-    def integrate(self, steps: int):
-        self._check(self._L.ladds_gpu_integrate(self._h, steps))
+    def integrate(self, steps: int, allow_nonfinite: bool = False) -> bool:
+        """Yoshida steps; with allow_nonfinite a state that became non-finite is
+        kept (returns False) for remove_escaping, as the reference loop does."""
+        rc = self._L.ladds_gpu_integrate(self._h, steps)
+        if allow_nonfinite and rc == ERR_NONFINITE:
+            return False
+        self._check(rc)
+        return True
 
     def conjunctions(self, dt_scan: float, cap: int | None = None):
         cap = 4096 if cap is None else cap
@@ -400,6 +408,17 @@ class Context:
         ids = self._removed_ids
         removed = C.c_size_t()
         self._check(self._L.ladds_gpu_remove_below(self._h, min_altitude, C.byref(removed), _p(ids), n))
+        return ids[: removed.value].copy()
+
+    def remove_escaping(self):
+        """Ids of the objects removed for leaving the container (non-finite
+        state or outside the box; ladds_gpu_remove_escaping)."""
+        n = self.size()
+        if getattr(self, "_removed_ids", None) is None or len(self._removed_ids) < max(n, 1):
+            self._removed_ids = np.empty(max(n, 1), dtype=np.uint64)
+        ids = self._removed_ids
+        removed = C.c_size_t()
+        self._check(self._L.ladds_gpu_remove_escaping(self._h, C.byref(removed), _p(ids), n))
         return ids[: removed.value].copy()
 
     def mark_deleted(self, slots):

@@ -279,6 +279,26 @@ __global__ void k_burnup_flags(const double *__restrict__ x, const double *__res
   if (below && (threadIdx.x & 31) == 0) atomicAdd(burnt, (unsigned)__popc(below));
 }
 
+// keep[j] = 0 for the objects that leave the container: a position or
+// velocity that is not finite, or a position outside [boxMin, boxMax]
+// (AutoPas::updateContainer's leaving particles, Simulation.cpp:314; a NaN
+// position is inside no box); aliveBySlot mirrors keep in slot order.
+__global__ void k_escape_flags(DevState s, int n, double3 lo, double3 hi, uint32_t *__restrict__ keep,
+                               uint32_t *__restrict__ aliveBySlot, unsigned *__restrict__ escaped) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t k = 1u;
+  if (j < n) {
+    const double x = s.x[j], y = s.y[j], z = s.z[j];
+    const bool inside = x >= lo.x && x <= hi.x && y >= lo.y && y <= hi.y && z >= lo.z && z <= hi.z;
+    const bool finiteV = isfinite(s.vx[j]) && isfinite(s.vy[j]) && isfinite(s.vz[j]);
+    k = (inside && finiteV) ? 1u : 0u;
+    keep[j] = k;
+    if (tagSlot(s.tag[j]) < (uint32_t)n) aliveBySlot[tagSlot(s.tag[j])] = k;
+  }
+  const unsigned out = __ballot_sync(0xffffffffu, k == 0u);
+  if (out && (threadIdx.x & 31) == 0) atomicAdd(escaped, (unsigned)__popc(out));
+}
+
 // keep[j] = 0 for the objects whose slot is marked (slotMark[slot] = 1);
 // aliveBySlot mirrors it in slot order.
 __global__ void k_slot_mark_flags(const uint32_t *__restrict__ tag, int n, const uint8_t *__restrict__ slotMark,

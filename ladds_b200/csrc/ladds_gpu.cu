@@ -593,10 +593,12 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
     // the largest separation a record or a near-band flag can have, with room for rounding
     const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
+    HalfShellRows rows;
+    buildHalfShellRows(rows, c->grid.reach, c->grid.cellSize, reach * reach);
     (buffer ? k_pair_candidates<LADDS_SCREEN_BUFFER>
             : k_pair_candidates<LADDS_SCREEN_LISTS>)<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
         c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF, reach * reach,
-        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, out);
+        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, rows, out);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
               : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(
@@ -1830,6 +1832,38 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
   if (!burnt) return LADDS_OK;  // nothing burns up: the state, its order and the captured graphs stay
+  if (removedIds) {  // ids of the removed objects, in slot order, before the compaction renumbers them
+    std::vector<uint32_t> alive(n);
+    std::vector<uint64_t> ids(n);
+    CK(cudaMemcpy(alive.data(), c->scratchC, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ids.data(), c->cur.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    size_t w = 0;
+    for (int i = 0; i < n && w < cap; ++i)
+      if (!alive[i]) removedIds[w++] = ids[i];
+  }
+  int rc = compactKept(c);
+  if (rc) return rc;
+  if (nRemoved) *nRemoved = (size_t)n - c->n;
+  return LADDS_OK;
+}
+
+int ladds_gpu_remove_escaping(ladds_gpu_ctx *c, size_t *nRemoved, uint64_t *removedIds, size_t cap) {
+  if (!c) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (nRemoved) *nRemoved = 0;
+  if (!c->n) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  const int n = (int)c->n;
+  const double3 lo = make_double3(c->cfg.boxMin[0], c->cfg.boxMin[1], c->cfg.boxMin[2]);
+  const double3 hi = make_double3(c->cfg.boxMax[0], c->cfg.boxMax[1], c->cfg.boxMax[2]);
+  unsigned *dOut = reinterpret_cast<unsigned *>(c->dCandNeed);  // scratch word (reset by every scan)
+  CK(cudaMemsetAsync(dOut, 0, sizeof(unsigned), c->st));
+  k_escape_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur, n, lo, hi, c->scratchA, c->scratchC, dOut);
+  unsigned escaped = 0;
+  CK(cudaMemcpyAsync(&escaped, dOut, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  if (!escaped) return LADDS_OK;  // nobody leaves: the state, its order and the captured graphs stay
   if (removedIds) {  // ids of the removed objects, in slot order, before the compaction renumbers them
     std::vector<uint32_t> alive(n);
     std::vector<uint64_t> ids(n);

@@ -83,7 +83,7 @@ __device__ __forceinline__ void rowWindow(uint32_t r2, uint32_t xlo, uint32_t xh
 
 // half-shell row q of a reach-R walk: the own row (dz, dy) = (0, 0), the rows
 // (0, 1..R), then (dz, -R..R) for dz = 1..R
-__device__ __forceinline__ void halfShellRowOf(int q, int R, int &dz, int &dy) {
+__host__ __device__ __forceinline__ void halfShellRowOf(int q, int R, int &dz, int &dy) {
   if (q <= R) {
     dz = 0;
     dy = q;
@@ -100,8 +100,9 @@ __device__ __forceinline__ void halfShellRowOf(int q, int R, int &dz, int &dy) {
 // the neighbour row (dy, dz) that can hold partners within sqrt(reachR2), -1
 // if none.  The corner rows and columns of the (2R+1)^3 block drop out for
 // R >= 3.
-__device__ __forceinline__ int rowHalfWidth(int dy, int dz, int R, double c2, double reachR2) {
-  const int b = max(abs(dy) - 1, 0), e = max(abs(dz) - 1, 0);
+__host__ __device__ __forceinline__ int rowHalfWidth(int dy, int dz, int R, double c2, double reachR2) {
+  const int b = (dy < 0 ? -dy : dy) > 1 ? (dy < 0 ? -dy : dy) - 1 : 0;
+  const int e = (dz < 0 ? -dz : dz) > 1 ? (dz < 0 ? -dz : dz) - 1 : 0;
   const double m = (double)(b * b + e * e) * c2;
   if (m > reachR2) return -1;
   int w = R;
@@ -237,9 +238,64 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
   }
 }
 
+// Half-shell rows of a scan: (dz, dy, x half-width w) of every neighbour row
+// that can hold partners within the scan's reach, own row first, packed as
+// dz | (dy + 128) << 8 | w << 16.  Built on the host per scan (the reach
+// depends on the scan's cutoff); grids with more rows than the table holds
+// (reach > 7) compute them in the kernel instead.
+constexpr int kHalfRowsMax = 128;
+struct HalfShellRows {
+  int32_t n;  // rows in e[], or -1: compute from the reach
+  uint32_t e[kHalfRowsMax];
+};
+
+__device__ __forceinline__ void halfRow(const HalfShellRows &tab, int q, int R, double c2, double reachR2, int &dz,
+                                        int &dy, int &w) {
+  if (tab.n >= 0) {
+    const uint32_t v = tab.e[q];
+    dz = (int)(v & 0xffu);
+    dy = (int)((v >> 8) & 0xffu) - 128;
+    w = (int)((v >> 16) & 0xffu);
+  } else {
+    halfShellRowOf(q, R, dz, dy);
+    w = rowHalfWidth(dy, dz, R, c2, reachR2);
+  }
+}
+
+inline void buildHalfShellRows(HalfShellRows &t, int R, double cellSize, double reachR2) {
+  const int nq = (R + 1) + R * (2 * R + 1);
+  const double c2 = cellSize * cellSize;
+  t.n = 0;
+  for (int q = 0; q < nq; ++q) {
+    int dz, dy;
+    halfShellRowOf(q, R, dz, dy);
+    const int w = rowHalfWidth(dy, dz, R, c2, reachR2);
+    if (w < 0) continue;
+    if (t.n == kHalfRowsMax || R > 127) {
+      t.n = -1;  // too many rows for the table: the kernel computes them
+      return;
+    }
+    t.e[t.n++] = (uint32_t)dz | ((uint32_t)(dy + 128) << 8) | ((uint32_t)w << 16);
+  }
+}
+
+constexpr int kWalkGroup = 8;        // neighbour rows whose windows are dealt out together
+constexpr uint32_t kDealPass = 1024;  // items of one dealing pass (32 mask words)
+
 // cutF: cutoff * (1 + nearRel) rounded up, so that every pair the exact gate or
-// its near band accepts passes the binary32 test.  The loops over the
-// neighbour rows are warp-uniform; inactive lanes contribute empty windows.
+// its near band accepts passes the binary32 test.
+//
+// One warp walks the half shells of 32 consecutive objects of the cell order.
+// Neighbour rows are taken kWalkGroup at a time: every lane locates its window
+// [lo, hi) in each row of the group (all lookups in flight together), and the
+// non-empty windows of the whole warp -- up to 32 x kWalkGroup -- are listed
+// in shared memory in item order, each with its offset lo - (first item) and
+// its owner lane.  The concatenated items are then dealt out 32 per round:
+// the windows that start inside a round are marked in a bit mask per round
+// (built once per pass with shared atomics), so the window of item i is
+// found as (windows started before the round) + popc(mask & lanes <= i) - 1,
+// one shared load instead of a search.  The objects' own binary32 positions
+// are staged in shared memory once.  Inactive lanes contribute empty windows.
 template <int SCREEN>
 __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__restrict__ tags,
                                                               const float4 *__restrict__ posf, int n,
@@ -248,8 +304,12 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
                                                               const uint16_t *__restrict__ cellOff, GridDesc g,
                                                               float cutF, double reachR2, uint32_t denseMin,
                                                               const uint32_t *__restrict__ denseCount,
-                                                              const CandSink out) {
-  __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
+                                                              const HalfShellRows rows, const CandSink out) {
+  constexpr int W = kScanCta / 32;
+  __shared__ uint2 sCand[W][kWarpCand];
+  __shared__ uint2 sWin[W][32 * kWalkGroup];  // (lo - first item, owner lane) by window rank
+  __shared__ uint32_t sMask[W][kDealPass / 32];
+  __shared__ float4 sOwn[W][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
   const int warpBase = blockIdx.x * kScanCta + warp * 32;
@@ -274,56 +334,144 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
       }
     }
   }
+  const float4 me = inRange ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  sOwn[warp][lane] = me;
   const double c2 = g.cellSize * g.cellSize;
   // Dense populations (the buffer form) with cells below the cutoff (reach >=
-  // 2): the object's own x-window in
-  // each neighbour row: partners lie within reachF of it, and a row whose
-  // (y, z) cell box is dyMin, dzMin away can hold them only within
-  // hw = sqrt(reachF^2 - dyMin^2 - dzMin^2) of its x.  Binary32 geometry with a
-  // 50 m margin over the pre-filter radius (which dwarfs the rounding of
-  // positions and cell edges); offsets inside the own cell are clamped to the
-  // cell, which only widens the windows of objects clamped into boundary
-  // cells.  With reach 1, or sparse populations (the list form), the cell
-  // windows are kept: trimming them does not pay for its arithmetic.
+  // 2): the object's own x-window in each neighbour row: partners lie within
+  // reachF of it, and a row whose (y, z) cell box is dyMin, dzMin away can
+  // hold them only within hw = sqrt(reachF^2 - dyMin^2 - dzMin^2) of its x.
+  // Binary32 geometry with a 50 m margin over the pre-filter radius (which
+  // dwarfs the rounding of positions and cell edges); offsets inside the own
+  // cell are clamped to the cell, which only widens the windows of objects
+  // clamped into boundary cells.
   const bool perObject = SCREEN == LADDS_SCREEN_BUFFER && R >= 2;  // warp-uniform
-  const float4 me = active && perObject ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
   const float cf = (float)g.cellSize, invCf = (float)g.invCell;
   const float fy = fminf(fmaxf(me.y - ((float)g.boxMin[1] + (float)iy * cf), 0.f), cf);
   const float fz = fminf(fmaxf(me.z - ((float)g.boxMin[2] + (float)iz * cf), 0.f), cf);
   const float xRel = me.x - (float)g.boxMin[0];
   const float reachF = cutF + 0.05f, reachF2 = reachF * reachF;
-  for (int dz = 0; dz <= R; ++dz) {
-    const float dzMin = dz == 0 ? 0.f : (float)(dz - 1) * cf + (cf - fz);
-    for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
-      const int w = rowHalfWidth(dy, dz, R, c2, reachR2);  // warp-uniform
-      if (w < 0) continue;
+  const int nq = rows.n >= 0 ? rows.n : (R + 1) + R * (2 * R + 1);
+  const uint32_t pitch = cellOffPitch((uint32_t)nx);
+  __syncwarp();
+  for (int q0 = 0; q0 < nq; q0 += kWalkGroup) {
+    const int gq = min(kWalkGroup, nq - q0);  // warp-uniform
+    uint32_t lo[kWalkGroup], cnt[kWalkGroup];
+#pragma unroll
+    for (int t = 0; t < kWalkGroup; ++t) {
+      lo[t] = 0u;
+      cnt[t] = 0u;
+      if (t >= gq) continue;
+      int dz, dy, w;
+      halfRow(rows, q0 + t, R, c2, reachR2, dz, dy, w);
+      const bool own = dz == 0 && dy == 0;
       const int32_t jz = iz + dz, jy = iy + dy;
-      int32_t lo32 = dz == 0 && dy == 0 ? ix : max(ix - w, 0), hi32 = min(ix + w, nx - 1);
-      bool inReach = true;
+      int32_t lo32 = own ? ix : max(ix - w, 0), hi32 = min(ix + w, nx - 1);
+      bool inReach = w >= 0;
       if (perObject) {
+        const float dzMin = dz == 0 ? 0.f : (float)(dz - 1) * cf + (cf - fz);
         const float dyMin =
             dy == 0 ? 0.f : dy > 0 ? (float)(dy - 1) * cf + (cf - fy) : (float)(-dy - 1) * cf + fy;
         const float h2 = reachF2 - dyMin * dyMin - dzMin * dzMin;
         const float hw = h2 > 0.f ? h2 * rsqrtf(h2) : 0.f;
-        if (!(dz == 0 && dy == 0)) lo32 = max(lo32, (int32_t)floorf((xRel - hw) * invCf));
+        if (!own) lo32 = max(lo32, (int32_t)floorf((xRel - hw) * invCf));
         hi32 = min(hi32, (int32_t)floorf((xRel + hw) * invCf));
-        inReach = h2 >= 0.f && hi32 >= lo32;
+        inReach = inReach && h2 >= 0.f && hi32 >= lo32;
       }
       const bool ok = active && jz < nz && jy >= 0 && jy < ny && inReach;
       const uint32_t r2 = ok ? (uint32_t)jz * (uint32_t)ny + (uint32_t)jy : 0u;
-      const uint32_t xlo = ok ? (uint32_t)lo32 : 0u;
-      const uint32_t xhi = ok ? (uint32_t)hi32 : 0u;
-      const RowLookup L = rowLoads(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff);  // four reads in flight
-      uint32_t lo = 0, hi = 0;
-      if (ok) {
-        rowFinish(L, r2, xlo, xhi, (uint32_t)nx, cellOff, skeys, lo, hi);
-        if (dz == 0 && dy == 0) {  // own cell: later objects only
-          lo = (uint32_t)j + 1u;
-          if (hi < lo) hi = lo;
-        }
+      const uint32_t xlo = ok ? (uint32_t)lo32 : 0u, xhi = ok ? (uint32_t)hi32 : 0u;
+      RowLookup L;
+      L.rs0 = __ldg(&rowStart[r2]);
+      L.rs1 = __ldg(&rowStart[r2 + 1]);
+      L.o0 = L.o1 = 0u;
+      if (cellOff) {
+        const uint16_t *tp = cellOff + (size_t)r2 * pitch;
+        L.o0 = __ldg(&tp[xlo]);
+        L.o1 = __ldg(&tp[xhi + 1]);
       }
-      warpWindowPairs<SCREEN>(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
+      if (ok) {
+        uint32_t a, b;
+        rowFinish(L, r2, xlo, xhi, (uint32_t)nx, cellOff, skeys, a, b);
+        if (own) {  // own cell: later objects only
+          a = (uint32_t)j + 1u;
+          if (b < a) b = a;
+        }
+        lo[t] = a;
+        cnt[t] = b - a;
+      }
     }
+    // item prefix and window rank of every lane (two warp scans in one)
+    uint32_t tot = 0, nonEmpty = 0;
+#pragma unroll
+    for (int t = 0; t < kWalkGroup; ++t) {
+      tot += cnt[t];
+      nonEmpty += cnt[t] ? 1u : 0u;
+    }
+    uint32_t inclT = tot, inclE = nonEmpty;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t a = __shfl_up_sync(0xffffffffu, inclT, o), b = __shfl_up_sync(0xffffffffu, inclE, o);
+      if (lane >= o) {
+        inclT += a;
+        inclE += b;
+      }
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inclT, 31);
+    if (total == 0u) continue;  // warp-uniform
+    // windows in item order: lane-major, rows in order inside a lane
+    {
+      uint32_t item = inclT - tot, rank = inclE - nonEmpty;
+#pragma unroll
+      for (int t = 0; t < kWalkGroup; ++t) {
+        if (cnt[t]) {
+          sWin[warp][rank] = make_uint2(lo[t] - item, (uint32_t)lane);
+          ++rank;
+        }
+        item += cnt[t];
+      }
+    }
+    for (uint32_t pass = 0; pass < total; pass += kDealPass) {  // warp-uniform
+      __syncwarp();
+      sMask[warp][lane] = 0u;
+      // windows started before the pass; marks of the windows starting inside it
+      uint32_t before = 0, item = inclT - tot;
+#pragma unroll
+      for (int t = 0; t < kWalkGroup; ++t) {
+        if (cnt[t]) {
+          if (item < pass) ++before;
+        }
+        item += cnt[t];
+      }
+      __syncwarp();
+      item = inclT - tot;
+#pragma unroll
+      for (int t = 0; t < kWalkGroup; ++t) {
+        if (cnt[t] && item >= pass && item - pass < kDealPass)
+          atomicOr(&sMask[warp][(item - pass) >> 5], 1u << ((item - pass) & 31u));
+        item += cnt[t];
+      }
+      uint32_t started = __reduce_add_sync(0xffffffffu, before);
+      __syncwarp();
+      const uint32_t end = min(total - pass, kDealPass);
+      for (uint32_t base = 0; base < end; base += 32u) {  // warp-uniform
+        const uint32_t mask = sMask[warp][base >> 5];
+        const uint32_t it = pass + base + (uint32_t)lane;
+        const bool valid = base + (uint32_t)lane < end;
+        const uint32_t rank = started + (uint32_t)__popc(mask & (0xffffffffu >> (31 - lane))) - 1u;
+        started += (uint32_t)__popc(mask);
+        bool pass2 = false;
+        uint32_t jj = 0u, k = 0u;
+        if (valid) {
+          const uint2 wv = sWin[warp][rank];
+          k = wv.x + it;
+          jj = (uint32_t)warpBase + wv.y;
+          pass2 = prefilterPass(sOwn[warp][wv.y], __ldg(&posf[k]), cutF);
+        }
+        warpAppend<SCREEN>(pass2, jj, k, lane, sCand[warp], nBuf, out);
+      }
+    }
+    __syncwarp();
   }
   warpFlush<SCREEN>(lane, sCand[warp], nBuf, out);
 }

@@ -3,7 +3,9 @@
 //   - after 100 iterations without a collision every parent id is reset
 //     (spawn protection, :291-293, :470-473);
 //   - integrate one step (:297);
-//   - delete burn-ups below minAltitude (:302, :561-596);
+//   - delete burn-ups below minAltitude (:302, :561-596) and particles that
+//     leave the container: outside the box or with a non-finite state (:314,
+//     :381-387);
 //   - every timestepsPerCollisionDetection iterations, the conjunction scan with
 //     dt = deltaT * k (:389-397), collisions / evasions handed to the writer.
 // The population stays on the device; the container is kept in step for
@@ -28,6 +30,7 @@ class HotPathLoop {
   void setCollisionWriter(Writer w) { writeCollisions_ = std::move(w); }
   void setEvasionWriter(Writer w) { writeEvasions_ = std::move(w); }
   size_t totalEvasions() const { return totalEvasions_; }
+  size_t escaped() const { return escaped_; }
   size_t iteration() const { return iteration_; }
 
  private:
@@ -36,7 +39,7 @@ class HotPathLoop {
   double deltaT_, minAltitude_, cutoff_, factor_, minDetectionRadius_, evasionCutoff_, conjunctionThreshold_;
   size_t k_;
   std::vector<uint64_t> removedIds_;  // ids of the iteration's burn-ups (kept between iterations)
-  size_t iteration_ = 0, iterationsSinceLastCollision_ = 0, totalEvasions_ = 0;
+  size_t iteration_ = 0, iterationsSinceLastCollision_ = 0, totalEvasions_ = 0, escaped_ = 0;
   Writer writeCollisions_, writeEvasions_;
 };
 

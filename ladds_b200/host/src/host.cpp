@@ -436,22 +436,29 @@ size_t HotPathLoop::run(size_t n) {
       gpu_.check(ladds_gpu_clear_parents(gpu_.handle()));
       for (auto &p : container_) p.setParentIdentifier(std::numeric_limits<size_t>::max());
     }
-    gpu_.check(ladds_gpu_integrate(gpu_.handle(), 1));
-    // burn-ups: removed on the device and, by id, from the container
-    const size_t before = gpu_.deviceSize();
-    if (removedIds_.size() < before) removedIds_.resize(before);  // reused: no population-sized buffer per iteration
-    std::vector<uint64_t> &removed = removedIds_;
-    size_t nRemoved = 0;
-    gpu_.check(ladds_gpu_remove_below(gpu_.handle(), minAltitude_, &nRemoved, removed.data(), before));
-    if (nRemoved) {
-      std::vector<uint64_t> gone(removed.begin(), removed.begin() + (std::ptrdiff_t)std::min(nRemoved, before));
-      std::sort(gone.begin(), gone.end());
-      container_.erase(std::remove_if(container_.begin(), container_.end(),
-                                      [&](const Particle &p) {
-                                        return std::binary_search(gone.begin(), gone.end(), (uint64_t)p.getID());
-                                      }),
-                       container_.end());
-      gpu_.markMirrored(container_);
+    // particles whose state became non-finite leave the container below
+    const int irc = ladds_gpu_integrate(gpu_.handle(), 1);
+    if (irc != LADDS_ERR_NONFINITE) gpu_.check(irc);
+    // burn-ups (Simulation.cpp:302) and particles leaving the container
+    // (:314, :381-387): removed on the device and, by id, from the container
+    for (int pass = 0; pass < 2; ++pass) {
+      const size_t before = gpu_.deviceSize();
+      if (removedIds_.size() < before) removedIds_.resize(before);  // reused: no population-sized buffer per iteration
+      std::vector<uint64_t> &removed = removedIds_;
+      size_t nRemoved = 0;
+      gpu_.check(pass == 0 ? ladds_gpu_remove_below(gpu_.handle(), minAltitude_, &nRemoved, removed.data(), before)
+                           : ladds_gpu_remove_escaping(gpu_.handle(), &nRemoved, removed.data(), before));
+      if (nRemoved) {
+        std::vector<uint64_t> gone(removed.begin(), removed.begin() + (std::ptrdiff_t)std::min(nRemoved, before));
+        std::sort(gone.begin(), gone.end());
+        container_.erase(std::remove_if(container_.begin(), container_.end(),
+                                        [&](const Particle &p) {
+                                          return std::binary_search(gone.begin(), gone.end(), (uint64_t)p.getID());
+                                        }),
+                         container_.end());
+        gpu_.markMirrored(container_);
+        if (pass == 1) escaped_ += nRemoved;
+      }
     }
     if (iteration_ % k_ == 0) {
       std::vector<ladds_pair> recs(1024);

@@ -371,6 +371,28 @@ def test_nonfinite_state_is_reported_and_rolled_back(capi):
         assert np.array_equal(back["x"], pop["x"]) and ctx.iteration() == 0
 
 
+def test_escaping_particles_leave_the_container(capi):
+    """Simulation.cpp:314, :381-387: after an integration, particles outside
+    the box and particles whose state became non-finite leave the container.
+    The integration keeps the non-finite state (LADDS_ERR_NONFINITE);
+    ladds_gpu_remove_escaping drops both kinds, the rest steps on."""
+    pop = capi.generate_population(0, 12, 2000)
+    pop["x"][3] = pop["y"][3] = pop["z"][3] = 0.0  # at the geocentre: 1/r -> inf
+    pop["x"][7], pop["y"][7], pop["z"][7] = 9999.0, 0.0, 0.0  # leaves the +-10000 km box within a step
+    pop["vx"][7], pop["vy"][7], pop["vz"][7] = 5.0, 0.0, 0.0
+    with ctx_for(capi) as ctx:
+        ctx.upload(pop)
+        assert ctx.remove_escaping().size == 0  # nothing leaves before the step
+        assert ctx.integrate(1, allow_nonfinite=True) is False
+        assert ctx.iteration() == 1
+        gone = ctx.remove_escaping()
+        assert sorted(gone.tolist()) == [3, 7] and ctx.size() == 1998
+        back = ctx.download()
+        assert np.all(np.isfinite(back["x"])) and not np.isin([3, 7], back["id"]).any()
+        ctx.step(2)  # the rest integrates and scans normally
+        assert ctx.remove_escaping().size == 0
+
+
 def test_burnup_removal_and_append(capi):
     pop = capi.generate_population(0, 6, 5000)
     low = capi.generate_population(0, 99, 100)
