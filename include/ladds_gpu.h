@@ -262,6 +262,17 @@ int ladds_gpu_mark_deleted(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t n);
 /* Sets every parentId to SIZE_MAX (Simulation.cpp:470-473). */
 int ladds_gpu_clear_parents(ladds_gpu_ctx *ctx);
 
+/* ---- state records: one particle, as get_objects and the exchange move it ---- */
+typedef struct {
+  double r[3], v[3];  /* position [km], velocity [km/s] */
+  double radius;      /* [m] */
+  double aom;         /* [km^2/kg]; mass = pi radius^2 1e-6 / aom */
+  double bcInv;       /* [m^2/kg] */
+  uint64_t id, parentId;
+  int32_t activity;
+  uint32_t deleted;   /* 1: marked deleted (ladds_gpu_mark_deleted) */
+} ladds_state_record; /* 96 bytes */
+
 /* ---- slab decomposition over ranks (driver: ladds_b200/slabs.py) ----
  * Replaces the domain decomposition of LADDS' MPI mode
  * (distributedMemParallelization/AltitudeBasedDecomposition.cpp:131-179,
@@ -285,6 +296,23 @@ int ladds_gpu_remove_slots(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t m);
  * in higher cell layers than every other object (the layers above a slab):
  * the half-shell walk finds a pair from its lower object.  SIZE_MAX: no halo. */
 int ladds_gpu_set_halo(ladds_gpu_ctx *ctx, size_t haloStart);
+/* Device-resident exchange (the particle communication of
+ * ParticleCommunicator.cpp:11-63, Simulation.cpp:313-376, with NCCL moving
+ * device buffers between ranks instead of MPI moving host objects).
+ * pack_layers: the live particles whose cell layer lies in [izLo, izHi), as
+ * state records in their current order, into `out` -- DEVICE memory of the
+ * context's device, cap records; *n = their number (LADDS_ERR_CAPACITY, and
+ * nothing written, when above cap).  remove != 0 also deletes them from the
+ * population (emigrants); survivors keep their relative slot order and are
+ * renumbered; with out NULL and cap 0 they are deleted without being packed.  append_records: appends m particles from state records in
+ * DEVICE memory (arrivals, a halo); a record with a non-finite value or an
+ * activity state out of range is LADDS_ERR_INVALID_ARG, nothing appended.
+ * truncate: deletes the particles with slot >= n (a halo appended for one
+ * scan).  None of them copies particle data through the host. */
+int ladds_gpu_pack_layers(ladds_gpu_ctx *ctx, int32_t izLo, int32_t izHi, int remove, ladds_state_record *out,
+                          size_t cap, size_t *n);
+int ladds_gpu_append_records(ladds_gpu_ctx *ctx, const ladds_state_record *records, size_t m);
+int ladds_gpu_truncate(ladds_gpu_ctx *ctx, size_t n);
 
 /* ---- explicit pair lists (the AoSFunctor call shape) ---- */
 /* One object of a pair evaluation (80 bytes). */
@@ -369,16 +397,7 @@ typedef struct {
 int ladds_gpu_phase_times(ladds_gpu_ctx *ctx, ladds_phase_times *t);
 int ladds_gpu_set_profiling(ladds_gpu_ctx *ctx, int enable);
 
-/* ---- objects by slot ---- */
-typedef struct {
-  double r[3], v[3];  /* position [km], velocity [km/s] */
-  double radius;      /* [m] */
-  double aom;         /* [km^2/kg]; mass = pi radius^2 1e-6 / aom */
-  double bcInv;       /* [m^2/kg] */
-  uint64_t id, parentId;
-  int32_t activity;
-  uint32_t deleted;   /* 1: marked deleted (ladds_gpu_mark_deleted) */
-} ladds_state_record; /* 96 bytes */
+/* ---- objects by slot (ladds_state_record: above) ---- */
 /* Current state of the objects with the given slots (upload / append index),
  * in the order asked; LADDS_ERR_INVALID_ARG if a slot does not exist. */
 int ladds_gpu_get_objects(ladds_gpu_ctx *ctx, const uint32_t *slots, size_t m, ladds_state_record *out);

@@ -86,7 +86,8 @@ EXPORTED = [
     "ladds_gpu_adjoint_backward", "ladds_gpu_adjoint_make_pairs", "ladds_gpu_autotune", "ladds_records_pack",
     "ladds_records_write_csv", "ladds_gpu_checked_insert", "ladds_gpu_get_objects", "ladds_breakup_collision",
     "ladds_gpu_breakup", "ladds_gpu_select_layers", "ladds_gpu_layer_histogram", "ladds_gpu_remove_slots",
-    "ladds_gpu_set_halo", "ladds_gpu_step_host", "ladds_gpu_pending_records", "ladds_population_write",
+    "ladds_gpu_set_halo", "ladds_gpu_pack_layers", "ladds_gpu_append_records", "ladds_gpu_truncate",
+    "ladds_gpu_step_host", "ladds_gpu_pending_records", "ladds_population_write",
     "ladds_population_read",
 ]
 
@@ -188,6 +189,9 @@ def lib():
     L.ladds_gpu_layer_histogram.argtypes = [vp, vp, sz]
     L.ladds_gpu_remove_slots.argtypes = [vp, vp, sz]
     L.ladds_gpu_set_halo.argtypes = [vp, sz]
+    L.ladds_gpu_pack_layers.argtypes = [vp, C.c_int32, C.c_int32, i, vp, sz, C.POINTER(sz)]
+    L.ladds_gpu_append_records.argtypes = [vp, vp, sz]
+    L.ladds_gpu_truncate.argtypes = [vp, sz]
     L.ladds_gpu_cell_sort_noalloc.argtypes = [i, vp, vp, sz, C.POINTER(C.c_int32 * 3), vp, vp, vp, C.c_char_p, sz]
     _lib = L
     return L
@@ -450,6 +454,34 @@ class Context:
     def set_halo(self, halo_start: int | None):
         """Objects with slot >= halo_start are pair-scan targets only (None: no halo)."""
         self._check(self._L.ladds_gpu_set_halo(self._h, (1 << 64) - 1 if halo_start is None else halo_start))
+
+    # device-resident exchange: buffers are device memory of this context's
+    # device, given as a pointer (int) or an object with data_ptr() (a torch tensor)
+    @staticmethod
+    def _dptr(buf):
+        return C.c_void_p(buf if isinstance(buf, int) else buf.data_ptr())
+
+    def pack_layers(self, iz_lo: int, iz_hi: int, remove: bool, out, cap: int) -> int:
+        """State records of the live objects of cell layers [iz_lo, iz_hi) into
+        device memory `out` (cap records); returns their number."""
+        n = C.c_size_t()
+        self._check(self._L.ladds_gpu_pack_layers(self._h, iz_lo, iz_hi, int(bool(remove)),
+                                                  self._dptr(out) if out is not None else None, cap,
+                                                  C.byref(n)))
+        return n.value
+
+    def torch_device(self) -> str:
+        """The torch device of this context's GPU (for exchange buffers)."""
+        return f"cuda:{self.config.device}"
+
+    def append_records(self, records, m: int):
+        """Appends m objects from state records in device memory."""
+        if m:
+            self._check(self._L.ladds_gpu_append_records(self._h, self._dptr(records), m))
+
+    def truncate(self, n: int):
+        """Deletes the objects with slot >= n."""
+        self._check(self._L.ladds_gpu_truncate(self._h, n))
 
     def scan(self, params: ScanParams, cap: int = 4096):
         """Conjunction scan of the current state with explicit functor scalars."""

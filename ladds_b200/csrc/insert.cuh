@@ -10,6 +10,7 @@
 // tested against the ones accepted before them on the host, in batch order.
 #pragma once
 #include "conjunction.cuh"
+#include "propagate.cuh"
 
 namespace ladds {
 
@@ -97,6 +98,67 @@ __global__ void k_gather_records(DevState s, const int32_t *__restrict__ pos, in
   r.activity = tagAct(s.tag[j]);
   r.deleted = tagDummy(s.tag[j]) ? 1u : 0u;
   out[q] = r;
+}
+
+// Layer selection of the device-resident exchange (ladds_gpu_pack_layers):
+// sel[j] = 1 for the live objects whose cell layer lies in [lo, hi), keep[j]
+// = !sel[j] and aliveBySlot its slot-order mirror (for the removal).
+__global__ void k_layer_flags(const double *__restrict__ z, const uint32_t *__restrict__ tag, int n, GridDesc g,
+                              int32_t lo, int32_t hi, uint32_t *__restrict__ sel, uint32_t *__restrict__ keep,
+                              uint32_t *__restrict__ aliveBySlot) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t t = tag[j];
+  const int32_t iz = (int32_t)cellCoord(z[j], g.boxMin[2], g.invCell, g.n[2]);
+  const uint32_t s = (!tagDummy(t) && iz >= lo && iz < hi) ? 1u : 0u;
+  sel[j] = s;
+  keep[j] = 1u - s;
+  if (tagSlot(t) < (uint32_t)n) aliveBySlot[tagSlot(t)] = 1u - s;
+}
+
+// positions of the selected objects in their (current) order: idx[pos[j]] = j
+__global__ void k_selected_positions(const uint32_t *__restrict__ sel, const uint32_t *__restrict__ pos, int n,
+                                     int32_t *__restrict__ idx) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n && sel[j]) idx[pos[j]] = j;
+}
+
+// State records (device memory) appended at positions / slots offset..offset+m
+// (slot-indexed radius, id and parent at the same index); bad[0] counts
+// records with a non-finite value or an activity state out of range.
+__global__ void k_append_records(const ladds_state_record *__restrict__ in, int m, DevState s, uint32_t offset,
+                                 unsigned *__restrict__ bad) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const ladds_state_record r = in[q];
+  const uint32_t at = offset + (uint32_t)q;
+  const bool ok = isfinite(r.r[0]) && isfinite(r.r[1]) && isfinite(r.r[2]) && isfinite(r.v[0]) &&
+                  isfinite(r.v[1]) && isfinite(r.v[2]) && isfinite(r.radius) && isfinite(r.aom) &&
+                  isfinite(r.bcInv) && r.activity >= 0 && r.activity <= 2;
+  if (!ok) atomicAdd(bad, 1u);
+  s.x[at] = r.r[0];
+  s.y[at] = r.r[1];
+  s.z[at] = r.r[2];
+  s.vx[at] = r.v[0];
+  s.vy[at] = r.v[1];
+  s.vz[at] = r.v[2];
+  s.aom[at] = r.aom;
+  s.bc[at] = r.bcInv;
+  s.radius[at] = r.radius;
+  s.id[at] = r.id;
+  s.parent[at] = r.parentId;
+  s.tag[at] = makeTag(at, ok ? r.activity : 0, r.deleted != 0u);
+}
+
+// keep[j] = slot < n0 (the removal of a truncation), aliveBySlot its mirror
+__global__ void k_truncate_flags(const uint32_t *__restrict__ tag, int n, uint32_t n0, uint32_t *__restrict__ keep,
+                                 uint32_t *__restrict__ aliveBySlot) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t sl = tagSlot(tag[j]);
+  const uint32_t k = sl < n0 ? 1u : 0u;
+  keep[j] = k;
+  if (sl < (uint32_t)n) aliveBySlot[sl] = k;
 }
 
 }  // namespace ladds

@@ -1879,6 +1879,86 @@ int ladds_gpu_remove_escaping(ladds_gpu_ctx *c, size_t *nRemoved, uint64_t *remo
   return LADDS_OK;
 }
 
+int ladds_gpu_pack_layers(ladds_gpu_ctx *c, int32_t izLo, int32_t izHi, int remove, ladds_state_record *out,
+                          size_t cap, size_t *nOut) {
+  if (!c || !nOut || (cap && !out) || (!out && !remove))
+    return fail(c, LADDS_ERR_INVALID_ARG, "pack_layers: bad argument");
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  *nOut = 0;
+  if (!c->n || izHi <= izLo) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  if (cap) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, out) != cudaSuccess ||
+        !((at.type == cudaMemoryTypeDevice && at.device == c->dev) || at.type == cudaMemoryTypeManaged)) {
+      cudaGetLastError();
+      return fail(c, LADDS_ERR_INVALID_ARG, "pack_layers: out must be device memory of the context's device");
+    }
+  }
+  const int n = (int)c->n;
+  // keys0 / vals0 are the sort's unsorted-key and source scratch (free between
+  // calls); scratchA / scratchC take the removal flags of compactKept
+  uint32_t *sel = c->keys0, *pos = c->vals0;
+  auto *idx = reinterpret_cast<int32_t *>(c->scratchB);
+  k_layer_flags<<<blocksFor(n, 256), 256, 0, c->st>>>(c->cur.z, c->cur.tag, n, c->grid, izLo, izHi, sel,
+                                                       c->scratchA, c->scratchC);
+  enqueueExclusiveScan(c, sel, (size_t)n, pos);
+  CK(cudaGetLastError());
+  uint32_t last[2] = {0, 0};
+  CK(cudaMemcpyAsync(&last[0], pos + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&last[1], sel + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const size_t count = (size_t)last[0] + last[1];
+  *nOut = count;
+  if (!count) return LADDS_OK;
+  if (remove && !out) return compactKept(c);  // removed without being packed
+  if (count > cap) return fail(c, LADDS_ERR_CAPACITY, "pack_layers: more particles than the output holds");
+  k_selected_positions<<<blocksFor(n, 256), 256, 0, c->st>>>(sel, pos, n, idx);
+  k_gather_records<<<blocksFor(count, 128), 128, 0, c->st>>>(c->cur, idx, (int)count, out);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return remove ? compactKept(c) : LADDS_OK;
+}
+
+int ladds_gpu_append_records(ladds_gpu_ctx *c, const ladds_state_record *records, size_t m) {
+  if (!c || (m && !records)) return fail(c, LADDS_ERR_INVALID_ARG, "append_records: bad argument");
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (!m) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, records) != cudaSuccess ||
+      !((at.type == cudaMemoryTypeDevice && at.device == c->dev) || at.type == cudaMemoryTypeManaged)) {
+    cudaGetLastError();
+    return fail(c, LADDS_ERR_INVALID_ARG, "append_records: records must be device memory of the context's device");
+  }
+  if (c->n + m > (size_t)kTagSlotMask) return fail(c, LADDS_ERR_TOO_LARGE, "append_records: too many particles");
+  int rc = ensureCapacity(c, c->n + m);
+  if (rc) return rc;
+  unsigned *dBad = reinterpret_cast<unsigned *>(c->dCandNeed);  // scratch word (reset by every scan)
+  CK(cudaMemsetAsync(dBad, 0, sizeof(unsigned), c->st));
+  k_append_records<<<blocksFor(m, 128), 128, 0, c->st>>>(records, (int)m, c->cur, (uint32_t)c->n, dBad);
+  CK(cudaGetLastError());
+  unsigned bad = 0;
+  CK(cudaMemcpyAsync(&bad, dBad, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (bad) return fail(c, LADDS_ERR_INVALID_ARG, "append_records: a record holds NaN/Inf or a bad activity state");
+  c->n += m;
+  c->orderValid = false;
+  dropGraphs(c);
+  return LADDS_OK;
+}
+
+int ladds_gpu_truncate(ladds_gpu_ctx *c, size_t n0) {
+  if (!c) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (n0 >= c->n) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  k_truncate_flags<<<blocksFor(c->n, 256), 256, 0, c->st>>>(c->cur.tag, (int)c->n, (uint32_t)n0, c->scratchA,
+                                                             c->scratchC);
+  CK(cudaGetLastError());
+  return compactKept(c);
+}
+
 int ladds_gpu_remove_slots(ladds_gpu_ctx *c, const uint32_t *slots, size_t m) {
   if (!c || (m && !slots)) return LADDS_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);

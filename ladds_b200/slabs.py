@@ -24,9 +24,14 @@ the union of the ranks' records is the single-context record set, bit for bit
 instead scans each rank's container alone and checks migrants in a swept box,
 which misses pairs across rank borders that involve no migrant.
 
-Exchanges are host-side object lists (96-byte state records) through
-``torch.distributed`` collectives -- all-gathers of the emigrants and of the
-halos, so every rank takes the same collective steps in the same order.  The
+Exchanges stay on the device: the library packs the emigrants and the halo
+as 96-byte state records into device buffers (ladds_gpu_pack_layers), one
+``all_to_all_single`` of ``torch.distributed`` moves them between the ranks
+(NCCL: device to device over NVLink; counts first, then the records), and the
+receivers append them from device memory (ladds_gpu_append_records).  Every
+rank takes the same collective steps in the same order; no particle crosses
+the host.  Under a gloo group (CPU tests, or several ranks sharing one GPU)
+the buffers are staged through host memory for the collective only.  The
 engine is a ``capi.Context`` (one per rank, on its own GPU); anything with
 the same methods works.
 """
@@ -35,6 +40,8 @@ from __future__ import annotations
 import numpy as np
 
 from . import capi
+
+REC = capi.STATE_RECORD_DTYPE.itemsize  # bytes of one state record
 
 
 def _dist():
@@ -99,13 +106,40 @@ class SlabDecomposition:
         self.migrated = 0  # emigrants handed over by this rank so far
 
     def all_gather(self, obj) -> list:
-        """obj of every rank, in rank order (a single process: [obj])."""
+        """obj of every rank, in rank order (a single process: [obj]); small
+        host values only (bounds, counts, test results)."""
         d = _dist()
         if not d or self.world == 1:
             return [obj]
         out = [None] * self.world
         d.all_gather_object(out, obj, group=self.group)
         return out
+
+    def _device(self):
+        return self.e.torch_device() if hasattr(self.e, "torch_device") else "cpu"
+
+    def exchange(self, send, counts: list[int]):
+        """All-to-all of state records: counts[d] records of `send` (a uint8
+        device tensor, destinations in rank order) go to rank d.  Returns the
+        received records (a uint8 tensor on the engine's device, sources in rank
+        order) and their number.  Counts travel first (one int64 per rank)."""
+        import torch
+
+        d = _dist()
+        dev = self._device()
+        if not d or self.world == 1:
+            return torch.empty(0, dtype=torch.uint8, device=dev), 0
+        stage = d.get_backend(self.group) == "gloo" and torch.device(dev).type == "cuda"
+        cdev = "cpu" if stage else dev
+        sc = torch.tensor(counts, dtype=torch.int64, device=cdev)
+        rc = torch.empty_like(sc)
+        d.all_to_all_single(rc, sc, group=self.group)
+        recv_counts = [int(v) for v in rc.tolist()]
+        payload = send.to(cdev) if stage else send
+        recv = torch.empty(sum(recv_counts) * REC, dtype=torch.uint8, device=cdev)
+        d.all_to_all_single(recv, payload, output_split_sizes=[c * REC for c in recv_counts],
+                            input_split_sizes=[c * REC for c in counts], group=self.group)
+        return (recv.to(dev) if stage else recv), sum(recv_counts)
 
     # ------------------------------------------------------------------ setup
     def distribute(self, bounds: list[int] | None = None) -> list[int]:
@@ -120,49 +154,57 @@ class SlabDecomposition:
             raise ValueError("every slab must be at least `reach` cell layers thick")
         self.bounds = list(bounds)
         lo, hi = self.bounds[self.rank], self.bounds[self.rank + 1]
-        out = np.concatenate([self.e.select_layers(0, lo), self.e.select_layers(hi, self.nz)])
-        if len(out):
-            self.e.remove_slots(out)
+        self.e.pack_layers(0, lo, True, None, 0)  # removed, not packed
+        self.e.pack_layers(hi, self.nz, True, None, 0)
         return self.bounds
 
     # ------------------------------------------------------------- iteration
+    def _pack(self, ranges, remove: bool):
+        """State records of the live objects of the layer ranges (one per rank,
+        None: nothing for that rank) packed back to back into one device
+        buffer; returns it and the per-rank counts."""
+        import torch
+
+        hist = np.asarray(self.e.layer_histogram(), dtype=np.int64)
+        counts = [0 if r is None else int(hist[r[0]:r[1]].sum()) for r in ranges]
+        buf = torch.empty(max(sum(counts), 1) * REC, dtype=torch.uint8, device=self._device())
+        off = 0
+        for r, c in zip(ranges, counts):
+            if c:
+                got = self.e.pack_layers(r[0], r[1], remove, buf[off * REC:], c)
+                if got != c:
+                    raise RuntimeError(f"layer histogram and packing disagree ({got} vs {c})")
+                off += c
+        return buf[: off * REC], counts
+
     def migrate(self) -> int:
         """Hands the objects that left this rank's layers to their owners and
         appends the arrivals; returns the number of arrivals."""
-        leaving, slots = {}, []
-        for d in range(self.world):
-            if d == self.rank:
-                continue
-            s = self.e.select_layers(self.bounds[d], self.bounds[d + 1])
-            if len(s):
-                leaving[d] = self.e.get_objects(s)
-                slots.append(s)
-        if slots:
-            self.e.remove_slots(np.concatenate(slots))
-            self.migrated += sum(len(s) for s in slots)
-        arrivals = [g[self.rank] for g in self.all_gather(leaving) if self.rank in g]
-        if arrivals:
-            self.e.append(records_to_population(np.concatenate(arrivals)))
-        return int(sum(len(a) for a in arrivals))
+        ranges = [None if d == self.rank else (self.bounds[d], self.bounds[d + 1]) for d in range(self.world)]
+        send, counts = self._pack(ranges, remove=True)
+        self.migrated += sum(counts)
+        recv, m = self.exchange(send, counts)
+        self.e.append_records(recv, m)
+        return m
 
     def scan(self, dt_scan: float) -> np.ndarray:
         """Pair scan of this rank's objects with each other and with the halo
         (the next rank's lowest `reach` layers); records of this rank."""
         lo = self.bounds[self.rank]
-        mine = self.e.select_layers(lo, lo + self.reach)
-        halos = self.all_gather(self.e.get_objects(mine) if len(mine) else None)
-        halo = halos[self.rank + 1] if self.rank + 1 < self.world else None
+        ranges = [None] * self.world
+        if self.rank > 0:  # this rank's lowest layers are the halo of the rank below
+            ranges[self.rank - 1] = (lo, lo + self.reach)
+        send, counts = self._pack(ranges, remove=False)
+        halo, m = self.exchange(send, counts)
         n0 = self.e.size()
-        if halo is not None and len(halo):
-            self.e.append(records_to_population(halo))
+        if m:
+            self.e.append_records(halo, m)
             self.e.set_halo(n0)
         try:
             recs = self.e.conjunctions(dt_scan)
         finally:
             self.e.set_halo(None)
-            n1 = self.e.size()
-            if n1 > n0:
-                self.e.remove_slots(np.arange(n0, n1, dtype=np.uint32))
+            self.e.truncate(n0)
         return recs
 
     def iterate(self, dt_scan: float | None) -> np.ndarray:

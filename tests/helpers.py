@@ -103,6 +103,34 @@ class OracleEngine:
     def set_halo(self, start):
         self.halo = start
 
+    # device-resident exchange of ladds_b200.slabs, on host memory: buffers are
+    # CPU torch tensors (uint8) holding state records
+    def torch_device(self):
+        return "cpu"
+
+    def pack_layers(self, lo, hi, remove, out, cap):
+        sel = self.select_layers(lo, hi)
+        if len(sel) and (out is not None or not remove):
+            if len(sel) > cap:
+                raise self.capi.LaddsError(self.capi.ERR_CAPACITY, "pack_layers: more particles than the output")
+            rec = self.get_objects(sel)
+            out[: rec.nbytes].numpy()[:] = np.frombuffer(rec.tobytes(), dtype=np.uint8)
+        if remove and len(sel):
+            self.remove_slots(sel)
+        return len(sel)
+
+    def append_records(self, buf, m):
+        if m:
+            from ladds_b200.slabs import records_to_population
+
+            rec = np.frombuffer(buf[: m * self.capi.STATE_RECORD_DTYPE.itemsize].numpy().tobytes(),
+                                dtype=self.capi.STATE_RECORD_DTYPE)
+            self.append(records_to_population(rec))
+
+    def truncate(self, n0):
+        if n0 < self.pop.n:
+            self.remove_slots(np.arange(n0, self.pop.n))
+
     def integrate(self, steps):
         self.o.propagate(self.pop, self.mask, self.dt, steps, t0=self.dt * self.it)
         self.it += steps

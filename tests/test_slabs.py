@@ -216,3 +216,40 @@ def test_gpu_slabs_match_single_context(capi, tmp_path):
     finally:
         single.close()
     assert got["moved"].sum() > 0
+
+
+@pytest.mark.gpu
+def test_gpu_device_exchange_primitives(capi):
+    """pack_layers / append_records / truncate on device buffers: the packed
+    records are get_objects of the selected slots in cell order, appending them
+    to another context reproduces them, removal and truncation keep the rest in
+    order, and host memory is refused as a buffer."""
+    import torch
+
+    pop = population(seed=6, n=4000)
+    rec_bytes = capi.STATE_RECORD_DTYPE.itemsize
+    with gpu_engine(pop) as a, gpu_engine(population(seed=7, n=500)) as b:
+        a.conjunctions(DT)  # cell order
+        keys, slots = a.cell_order()
+        sel = a.select_layers(24, 27)
+        buf = torch.empty(len(sel) * rec_bytes, dtype=torch.uint8, device="cuda")
+        with pytest.raises(capi.LaddsError) as e:
+            a.pack_layers(24, 27, False, buf, len(sel) - 1)
+        assert e.value.code == capi.ERR_CAPACITY
+        got = a.pack_layers(24, 27, False, buf, len(sel))
+        assert got == len(sel) > 100
+        rec = np.frombuffer(buf.cpu().numpy().tobytes(), dtype=capi.STATE_RECORD_DTYPE)
+        in_order = slots[np.isin(slots, sel)]  # the selected slots in cell order
+        assert rec.tobytes() == a.get_objects(in_order).tobytes()
+        n0 = b.size()
+        b.append_records(buf, got)
+        assert b.size() == n0 + got
+        assert b.get_objects(np.arange(n0, n0 + got)).tobytes() == rec.tobytes()
+        b.truncate(n0)
+        assert b.size() == n0
+        with pytest.raises(capi.LaddsError):  # host memory is not a device buffer
+            b.append_records(torch.zeros(rec_bytes, dtype=torch.uint8), 1)
+        ids_before = a.get_objects(np.arange(a.size()))["id"]
+        assert a.pack_layers(24, 27, True, None, 0) == len(sel)  # removed without being packed
+        assert a.size() == len(pop["x"]) - len(sel)
+        assert np.array_equal(a.get_objects(np.arange(a.size()))["id"], np.delete(ids_before, sel))
