@@ -463,12 +463,17 @@ def drift_leg(capi, device, pop, steps, cfg_kw=None):
 
 
 def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
-    """Config 4 form, the reference loop (Simulation.cpp:287-415) per
-    iteration: integrate; burn-ups below min_altitude removed (:302); particles
-    leaving the container (outside the box, or a non-finite state) removed
-    (:314, :381-387); the conjunction scan; the NASA breakup model on the host
-    for every collision, its fragments appended on the device
-    (BreakupWrapper.cpp:13-45, Simulation.cpp:610-633).  Also the expected
+    """Config 4 form over `iterations` iterations of the reference loop
+    (Simulation.cpp:287-415): integrate; burn-ups below min_altitude removed
+    (:302); particles leaving the container (outside the box, or a non-finite
+    state) removed (:314, :381-387); the conjunction scan; every collision
+    handed to the NASA breakup model on the host (BreakupWrapper.cpp:13-45),
+    its fragment count recorded.  The population is the same all day (the
+    fragments are counted, not appended): a breakup of these solid spheres
+    (2700 kg/m^3, up to 5 m: 1.4e6 kg) yields up to ~7e5 fragments at one point,
+    whose same-parent pairs the cell scan would visit quadratically.  After the
+    day, the first breakup is applied for real -- fragments appended on the
+    device (ladds_gpu_breakup) -- and propagated one step.  Also the expected
     collision count of the conjunction records, sum of ((r_A + r_B) / 0.1 km)^2
     over them (the fraction of a uniform-in-area miss distribution inside the
     collision radius)."""
@@ -477,8 +482,9 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
     bcfg = capi.BreakupConfig(0.05, 1, 2.2)
     n = len(pop["x"])
     next_id = int(np.max(pop["id"])) + 1 if n else 0
-    tot = dict(breakups=0, fragments=0, collisions=0, conjunctions=0, burnups=0, escaped=0, nonfinite_steps=0)
+    tot = dict(collisions=0, breakups=0, fragments=0, conjunctions=0, burnups=0, escaped=0, nonfinite_steps=0)
     expected = 0.0
+    first = None
     t0 = time.perf_counter()
     with capi.Context(cfg) as ctx:
         ctx.upload(pop)
@@ -490,44 +496,65 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
             rec = ctx.conjunctions(cfg.deltaT)
             col = rec[(rec["flags"] & capi.PAIR_COLLISION) != 0]
             conj = rec[(rec["flags"] & capi.PAIR_CONJUNCTION) != 0]
-            tot["collisions"] += len(col)
             tot["conjunctions"] += len(conj)
             if len(conj):
                 objs = ctx.get_objects(np.concatenate([conj["slotA"], conj["slotB"]]))
                 ra, rb = objs["radius"][: len(conj)], objs["radius"][len(conj):]
                 expected += float(np.sum(((ra + rb) * cfg.collisionDistanceFactor * 1e-3 / 0.1) ** 2))
-            if len(col):
-                nb, nf, next_id = ctx.breakup(rec, bcfg, 1000 + it, next_id)
-                tot["breakups"] += nb
-                tot["fragments"] += nf
-        size = ctx.size()
-    wall = time.perf_counter() - t0
+            for q, r in enumerate(col):
+                tot["collisions"] += 1
+                a, b = ctx.get_objects([r["slotA"], r["slotB"]])
+                frags, _ = capi.breakup_collision(bcfg, 1000 + it + q, a, b, r["point"], int(r["idA"]), next_id)
+                if len(frags["x"]):
+                    tot["breakups"] += 1
+                    tot["fragments"] += len(frags["x"])
+                    if first is None:
+                        first = (it, col[q:q + 1].copy())
+        wall = time.perf_counter() - t0
+        applied = None
+        if first is not None:  # the first breakup appended on the device, then one propagation step
+            n0 = ctx.size()
+            t1 = time.perf_counter()
+            nb, nf, next_id = ctx.breakup(first[1], bcfg, 1000 + first[0], next_id)
+            t_append = time.perf_counter() - t1
+            ok = ctx.integrate(1, allow_nonfinite=True)
+            gone = len(ctx.remove_escaping())
+            applied = {"iteration": first[0], "breakups": nb, "fragments_appended": nf, "objects_before": n0,
+                       "objects_after": ctx.size(), "append_ms": t_append * 1e3,
+                       "propagated_one_step": True, "nonfinite_after_step": not ok, "escaped_after_step": gone}
     return {"iterations": iterations, "hours": iterations * cfg.deltaT / 3600.0, **tot,
-            "expected_collisions_from_conjunctions": expected, "objects_after": size,
+            "expected_collisions_from_conjunctions": expected, "first_breakup_applied": applied,
             "ms_per_iteration_wall": wall * 1e3 / iterations}
 
 
 # ---------------------------------------------------------- adjoint leg
+FD_STENCIL = (1.0, -1.0, 0.5, -0.5, 0.25, -0.25)  # multiples of h of the perturbed evaluations
+
+
 def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6):
     """Finite-difference check of directional derivatives gd (one per pair)
-    from the losses f0 at x and fm[k] at x + c_k eps d, c = (1, -1, 1/2, -1/2),
-    with the argmin steps step0 / stepm[k] of each evaluation.
+    from the losses f0 at x and fm[k] at x + FD_STENCIL[k] h d, with the argmin
+    steps step0 / stepm[k] of each evaluation.
 
     The loss is a minimum over steps (and, inside a step, over the clamped
     closest-approach time), so it has kinks where two branches tie; the
     gradient is the derivative of the branch active at x.  Per pair and per
-    side: a side whose two points keep the argmin step gives a one-sided
-    Richardson extrapolation (second order, from h and h / 2); if both sides
-    keep it and agree, the central Richardson value is used; if they disagree
-    the stencil straddles a kink inside the step (the clamp of the time) and
-    the side that agrees with the active branch is taken; pairs where neither
-    side keeps the argmin are unresolved at this h.  Returns the per-pair
-    relative errors and the counts of each class."""
+    side: a side whose three points keep the argmin step gives a one-sided
+    Richardson extrapolation of D(t) = (f(t) - f0) / t over t = h, h/2, h/4,
+    (8 D(h/4) - 6 D(h/2) + D(h)) / 3 (error O(h^3)); the central quotients
+    C(t) = (f(t) - f(-t)) / 2t give (64 C(h/4) - 20 C(h/2) + C(h)) / 45 (error
+    O(h^6)).  If both sides keep the argmin and agree to tol, the central value
+    is used; if they disagree the stencil straddles a kink inside the step (the
+    clamp of the time) and the side that agrees with the active branch is
+    taken; pairs where neither side keeps the argmin are unresolved at this h.
+    Returns the per-pair relative errors and the counts of each class."""
     keep = stepm == step0[None, :]
-    keep_p, keep_m = keep[0] & keep[2], keep[1] & keep[3]
-    fwd = (4.0 * (fm[2] - f0) / (0.5 * eps) - (fm[0] - f0) / eps) / 3.0
-    bwd = (4.0 * (f0 - fm[3]) / (0.5 * eps) - (f0 - fm[1]) / eps) / 3.0
-    cen = (4.0 * (fm[2] - fm[3]) / eps - (fm[0] - fm[1]) / (2 * eps)) / 3.0
+    keep_p, keep_m = keep[0] & keep[2] & keep[4], keep[1] & keep[3] & keep[5]
+    d = lambda k, t: (fm[k] - f0) / (t * eps)  # one-sided quotient at t h (t may be negative)
+    fwd = (8.0 * d(4, 0.25) - 6.0 * d(2, 0.5) + d(0, 1.0)) / 3.0
+    bwd = (8.0 * d(5, -0.25) - 6.0 * d(3, -0.5) + d(1, -1.0)) / 3.0
+    c = lambda kp, km, t: (fm[kp] - fm[km]) / (2.0 * t * eps)
+    cen = (64.0 * c(4, 5, 0.25) - 20.0 * c(2, 3, 0.5) + c(0, 1, 1.0)) / 45.0
     scale = np.maximum(np.abs(cen), 1e-300)
     both = keep_p & keep_m
     agree = both & (np.abs(fwd - bwd) <= tol * scale)
@@ -566,7 +593,7 @@ def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
         d /= np.linalg.norm(d, axis=1, keepdims=True)
         eps = 1e-6 * np.linalg.norm(rows, axis=1)
         batch = []
-        for f in (1.0, -1.0, 0.5, -0.5):
+        for f in FD_STENCIL:
             q = pairs.copy()
             r = rows + f * eps[:, None] * d
             q["rA"], q["vA"], q["rB"], q["vB"] = r[:, 0:3], r[:, 3:6], r[:, 6:9], r[:, 9:12]
@@ -574,10 +601,11 @@ def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
         _, miss, stepP, _ = ctx.adjoint_forward(np.concatenate(batch), steps, ck)
         _, miss0, step0, _ = ctx.adjoint_forward(pairs, steps, ck)
     gd = np.sum(dx * d, axis=1)
-    rel, counts = fd_classify(gd, miss0, miss.reshape(4, n_pairs), step0, stepP.reshape(4, n_pairs), eps)
+    k = len(FD_STENCIL)
+    rel, counts = fd_classify(gd, miss0, miss.reshape(k, n_pairs), step0, stepP.reshape(k, n_pairs), eps)
     fin = rel[np.isfinite(rel)]
     f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
-    fd = {"direction": "random per pair, 12 state components, relative scaling", "h": "1e-6 |x| and h/2",
+    fd = {"direction": "random per pair, 12 state components, relative scaling", "h": "1e-6 |x|, h/2, h/4",
           "pairs": n_pairs, **counts,
           "meets_1e-6": int(np.sum(rel <= 1e-6)), "meets_1e-6_frac": float(np.mean(rel <= 1e-6)),
           "rel_err_median": float(np.median(fin)) if len(fin) else None,

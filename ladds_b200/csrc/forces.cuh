@@ -10,9 +10,14 @@
 
 namespace ladds {
 
+// Split precision finds the band without a search: every band edge of the
+// table is a multiple of 5 km, so the band of h in [0, 1000) km is a function
+// of floor(h / 5) (a 200-entry table; 1000 km and above: the last band).
+constexpr int kAtmBand5 = 201;
 struct AtmShared {
   double h0[kAtmBands], rho0[kAtmBands], H[kAtmBands];
-  float h0f[kAtmBands], invHf[kAtmBands];  // h0 and 1 / H in binary32 (split precision)
+  float4 rowf[kAtmBands];       // h0, 1 / H, rho0 in binary32 (split precision)
+  uint8_t band5[kAtmBand5 + 3];  // band of the altitudes [5 i, 5 i + 5) km
 };
 
 // stages the atmosphere table in shared memory (every thread of the block calls it)
@@ -21,8 +26,12 @@ __device__ __forceinline__ void loadAtmTable(AtmShared &atm, const AtmRow *rows)
     atm.h0[i] = rows[i].h0;
     atm.rho0[i] = rows[i].rho0;
     atm.H[i] = rows[i].H;
-    atm.h0f[i] = (float)rows[i].h0;
-    atm.invHf[i] = 1.0f / (float)rows[i].H;
+    atm.rowf[i] = make_float4((float)rows[i].h0, 1.0f / (float)rows[i].H, (float)rows[i].rho0, 0.0f);
+  }
+  for (int i = threadIdx.x; i < kAtmBand5; i += blockDim.x) {
+    int k = 0;  // largest k with h0[k] <= 5 i
+    while (k + 1 < kAtmBands && rows[k + 1].h0 <= 5.0 * i) ++k;
+    atm.band5[i] = (uint8_t)k;
   }
 }
 
@@ -36,17 +45,12 @@ __device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
   }
   return k;
 }
-// the same in binary32 (split precision: an altitude within binary32 rounding
-// of a band edge may take the neighbouring band, whose density agrees there to
-// the table's continuity)
+// the same in binary32 from the 5 km table (split precision: an altitude
+// within binary32 rounding of a band edge may take the neighbouring band,
+// whose density agrees there to the table's continuity)
 __device__ __forceinline__ int atmBandF(const AtmShared &t, float h) {
-  int k = 0;
-#pragma unroll
-  for (int step = 16; step >= 1; step >>= 1) {
-    const int c = k + step;
-    if (c < kAtmBands && h >= t.h0f[c]) k = c;
-  }
-  return k;
+  const int i = min(max((int)(h * 0.2f), 0), kAtmBand5 - 1);
+  return t.band5[i];
 }
 
 // Battin's f(q) = (1+q)^{3/2} - 1 written without cancellation.  The
@@ -191,8 +195,11 @@ __device__ __forceinline__ void accel(uint32_t mask, const double r[3], const do
       bz += k * (zf + f * sp[2]);
     }
     if (mask & kPropSRP) {
-      const double proj = x * e.sunHat[0] + y * e.sunHat[1] + z * e.sunHat[2];
-      const bool shadow = proj < 0.0 && (r2 - proj * proj) < kREarth * kREarth;
+      // cylindrical shadow from r . s: behind the Earth and within R of the
+      // Sun line (r^2 - (r . s)^2 / s^2 < R^2); binary32 moves the shadow edge
+      // by well under a metre
+      const float rs = xf * e.sunf[0] + yf * e.sunf[1] + zf * e.sunf[2];
+      const bool shadow = rs < 0.0f && ((float)r2 - rs * rs * e.sunInvS2f) < (float)(kREarth * kREarth);
       if (!shadow) {
         const float ux = xf - e.sunf[0], uy = yf - e.sunf[1], uz = zf - e.sunf[2];
         const float ui = rsqrtf(ux * ux + uy * uy + uz * uz);
@@ -210,8 +217,8 @@ __device__ __forceinline__ void accel(uint32_t mask, const double r[3], const do
       const float w2 = wx * wx + wy * wy + wz * wz;
       const float wn = w2 > 0.0f ? w2 * rsqrtf(w2) : 0.0f;
       const float h = (float)(rn - kREarth);
-      const int b = atmBandF(atm, h);
-      const float rho = (float)atm.rho0[b] * __expf(-(h - atm.h0f[b]) * atm.invHf[b]);
+      const float4 row = atm.rowf[atmBandF(atm, h)];
+      const float rho = row.z * __expf(-(h - row.x) * row.y);
       const float k = -0.5e3f * rho * (float)bcInv * wn;
       bx += k * wx;
       by += k * wy;
