@@ -531,7 +531,7 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
 FD_STENCIL = (1.0, -1.0, 0.5, -0.5, 0.25, -0.25)  # multiples of h of the perturbed evaluations
 
 
-def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6):
+def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3):
     """Finite-difference check of directional derivatives gd (one per pair)
     from the losses f0 at x and fm[k] at x + FD_STENCIL[k] h d, with the argmin
     steps step0 / stepm[k] of each evaluation.
@@ -541,18 +541,27 @@ def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6):
     gradient is the derivative of the branch active at x.  Per pair and per
     side: a side whose three points keep the argmin step gives a one-sided
     Richardson extrapolation of D(t) = (f(t) - f0) / t over t = h, h/2, h/4,
-    (8 D(h/4) - 6 D(h/2) + D(h)) / 3 (error O(h^3)); the central quotients
+    (8 D(h/4) - 6 D(h/2) + D(h)) / 3 (error O(h^3)), provided its two
+    second-order estimates 2 D(h/2) - D(h) and 2 D(h/4) - D(h/2) agree to
+    `consistency` (a kink inside the step -- the clamp of the closest-approach
+    time -- between the side's points breaks that); the central quotients
     C(t) = (f(t) - f(-t)) / 2t give (64 C(h/4) - 20 C(h/2) + C(h)) / 45 (error
-    O(h^6)).  If both sides keep the argmin and agree to tol, the central value
-    is used; if they disagree the stencil straddles a kink inside the step (the
-    clamp of the time) and the side that agrees with the active branch is
-    taken; pairs where neither side keeps the argmin are unresolved at this h.
-    Returns the per-pair relative errors and the counts of each class."""
+    O(h^6)).  Both sides usable and agreeing to tol: the central value.  Both
+    usable but disagreeing: a kink within h/4 of x, on an unknown side
+    ("ambiguous", the closer side's error is reported).  One side usable: that
+    side.  Neither: unresolved at this h.  Returns the per-pair relative
+    errors and the counts of each class."""
     keep = stepm == step0[None, :]
-    keep_p, keep_m = keep[0] & keep[2] & keep[4], keep[1] & keep[3] & keep[5]
     d = lambda k, t: (fm[k] - f0) / (t * eps)  # one-sided quotient at t h (t may be negative)
-    fwd = (8.0 * d(4, 0.25) - 6.0 * d(2, 0.5) + d(0, 1.0)) / 3.0
-    bwd = (8.0 * d(5, -0.25) - 6.0 * d(3, -0.5) + d(1, -1.0)) / 3.0
+    # a side is usable when its three points keep the argmin step and its two
+    # second-order estimates agree (a clamp kink inside the step breaks them)
+    r1p, r2p = 2.0 * d(2, 0.5) - d(0, 1.0), 2.0 * d(4, 0.25) - d(2, 0.5)
+    r1m, r2m = 2.0 * d(3, -0.5) - d(1, -1.0), 2.0 * d(5, -0.25) - d(3, -0.5)
+    fwd, bwd = (4.0 * r2p - r1p) / 3.0, (4.0 * r2m - r1m) / 3.0
+    smooth_p = np.abs(r1p - r2p) <= consistency * np.maximum(np.abs(r2p), 1e-300)
+    smooth_m = np.abs(r1m - r2m) <= consistency * np.maximum(np.abs(r2m), 1e-300)
+    keep_p = keep[0] & keep[2] & keep[4] & smooth_p
+    keep_m = keep[1] & keep[3] & keep[5] & smooth_m
     c = lambda kp, km, t: (fm[kp] - fm[km]) / (2.0 * t * eps)
     cen = (64.0 * c(4, 5, 0.25) - 20.0 * c(2, 3, 0.5) + c(0, 1, 1.0)) / 45.0
     scale = np.maximum(np.abs(cen), 1e-300)
@@ -567,7 +576,7 @@ def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6):
     rel[only_p] = err(fwd)[only_p]
     rel[only_m] = err(bwd)[only_m]
     unresolved = ~keep_p & ~keep_m
-    counts = {"central": int(agree.sum()), "kink_inside_step": int(kink.sum()), "forward_only": int(only_p.sum()),
+    counts = {"central": int(agree.sum()), "ambiguous": int(kink.sum()), "forward_only": int(only_p.sum()),
               "backward_only": int(only_m.sum()), "unresolved": int(unresolved.sum())}
     return rel, counts
 

@@ -332,16 +332,34 @@ __device__ __forceinline__ void sortOneRow(uint32_t r, uint32_t s0, uint32_t L, 
     }
     uint32_t run = incl - sum;
     const bool listDense = cellOff && dense.cells && L >= dense.minCount;
-    for (uint32_t i = 0; i < per; ++i) {
-      const uint32_t c = run0[i];
-      run0[i] = run;
-      run += c;
-      if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * per + i);  // counts past nx are 0
-    }
-    __syncwarp();
-    if (cellOff) {
-      uint16_t *t = cellOff + (size_t)r * pitch;
-      for (uint32_t c = lane; c <= nx; c += 32) t[c] = (uint16_t)hist[at(c)];
+    if (per == 8u && cellOff && 8u * 32u <= pitch) {
+      // the lane's eight exclusive prefixes are its eight cell-table entries:
+      // one 16-byte store (rows start on 16-byte boundaries; entries past nx
+      // are padding, written but never read)
+      uint32_t v[8];
+#pragma unroll
+      for (uint32_t i = 0; i < 8u; ++i) {
+        const uint32_t c = run0[i];
+        v[i] = run;
+        run0[i] = run;
+        run += c;
+        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * 8u + i);
+      }
+      *reinterpret_cast<uint4 *>(cellOff + (size_t)r * pitch + lane * 8u) =
+          make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
+      __syncwarp();
+    } else {
+      for (uint32_t i = 0; i < per; ++i) {
+        const uint32_t c = run0[i];
+        run0[i] = run;
+        run += c;
+        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * per + i);  // counts past nx are 0
+      }
+      __syncwarp();
+      if (cellOff) {
+        uint16_t *t = cellOff + (size_t)r * pitch;
+        for (uint32_t c = lane; c <= nx; c += 32) t[c] = (uint16_t)hist[at(c)];
+      }
     }
     for (uint32_t e = lane; e < L; e += 32) {  // place in cell order (arrival order inside a cell)
       const uint32_t ia = inIxArr[e], ix = ia & 0xffffu;

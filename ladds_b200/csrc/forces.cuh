@@ -195,11 +195,11 @@ __device__ __forceinline__ void accel(uint32_t mask, const double r[3], const do
       bz += k * (zf + f * sp[2]);
     }
     if (mask & kPropSRP) {
-      // cylindrical shadow from r . s: behind the Earth and within R of the
-      // Sun line (r^2 - (r . s)^2 / s^2 < R^2); binary32 moves the shadow edge
-      // by well under a metre
-      const float rs = xf * e.sunf[0] + yf * e.sunf[1] + zf * e.sunf[2];
-      const bool shadow = rs < 0.0f && ((float)r2 - rs * rs * e.sunInvS2f) < (float)(kREarth * kREarth);
+      // the shadow edge in binary64: it switches the whole SRP term, and a
+      // binary32 edge (~0.4 m) flips stage evaluations near it, which moved
+      // single objects by up to 0.3 m per day against the FP64 path
+      const double proj = x * e.sunHat[0] + y * e.sunHat[1] + z * e.sunHat[2];
+      const bool shadow = proj < 0.0 && (r2 - proj * proj) < kREarth * kREarth;
       if (!shadow) {
         const float ux = xf - e.sunf[0], uy = yf - e.sunf[1], uz = zf - e.sunf[2];
         const float ui = rsqrtf(ux * ux + uy * uy + uz * uz);

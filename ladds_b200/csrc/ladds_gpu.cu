@@ -595,10 +595,15 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
     HalfShellRows rows;
     buildHalfShellRows(rows, c->grid.reach, c->grid.cellSize, reach * reach);
-    (buffer ? k_pair_candidates<LADDS_SCREEN_BUFFER>
-            : k_pair_candidates<LADDS_SCREEN_LISTS>)<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(
-        c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF, reach * reach,
-        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount, rows, out);
+    const bool r1 = c->grid.reach == 1 && rows.n == 5;  // the five reach-1 rows, all of half-width 1
+    auto walk = buffer ? (r1 ? k_pair_candidates<LADDS_SCREEN_BUFFER, true>
+                             : k_pair_candidates<LADDS_SCREEN_BUFFER, false>)
+                       : (r1 ? k_pair_candidates<LADDS_SCREEN_LISTS, true>
+                             : k_pair_candidates<LADDS_SCREEN_LISTS, false>);
+    walk<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart,
+                                                        c->cellOff, c->grid, cutF, reach * reach,
+                                                        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount,
+                                                        rows, out);
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
               : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(

@@ -296,7 +296,10 @@ constexpr uint32_t kDealPass = 1024;  // items of one dealing pass (32 mask word
 // found as (windows started before the round) + popc(mask & lanes <= i) - 1,
 // one shared load instead of a search.  The objects' own binary32 positions
 // are staged in shared memory once.  Inactive lanes contribute empty windows.
-template <int SCREEN>
+// R1: reach-1 grids, whose half shell is the five rows (dz, dy) = (0, 0),
+// (0, 1), (1, -1), (1, 0), (1, 1), each with x half-width 1, known at compile
+// time (one group of five windows, no row table).
+template <int SCREEN, bool R1>
 __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__restrict__ tags,
                                                               const float4 *__restrict__ posf, int n,
                                                               const uint32_t *__restrict__ skeys,
@@ -306,8 +309,9 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
                                                               const uint32_t *__restrict__ denseCount,
                                                               const HalfShellRows rows, const CandSink out) {
   constexpr int W = kScanCta / 32;
+  constexpr int G = R1 ? 5 : kWalkGroup;  // windows per lane and group
   __shared__ uint2 sCand[W][kWarpCand];
-  __shared__ uint2 sWin[W][32 * kWalkGroup];  // (lo - first item, owner lane) by window rank
+  __shared__ uint2 sWin[W][32 * G];  // (lo - first item, owner lane) by window rank
   __shared__ uint32_t sMask[W][kDealPass / 32];
   __shared__ float4 sOwn[W][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -345,25 +349,31 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
   // dwarfs the rounding of positions and cell edges); offsets inside the own
   // cell are clamped to the cell, which only widens the windows of objects
   // clamped into boundary cells.
-  const bool perObject = SCREEN == LADDS_SCREEN_BUFFER && R >= 2;  // warp-uniform
+  const bool perObject = !R1 && SCREEN == LADDS_SCREEN_BUFFER && R >= 2;  // warp-uniform
   const float cf = (float)g.cellSize, invCf = (float)g.invCell;
   const float fy = fminf(fmaxf(me.y - ((float)g.boxMin[1] + (float)iy * cf), 0.f), cf);
   const float fz = fminf(fmaxf(me.z - ((float)g.boxMin[2] + (float)iz * cf), 0.f), cf);
   const float xRel = me.x - (float)g.boxMin[0];
   const float reachF = cutF + 0.05f, reachF2 = reachF * reachF;
-  const int nq = rows.n >= 0 ? rows.n : (R + 1) + R * (2 * R + 1);
+  const int nq = R1 ? 5 : rows.n >= 0 ? rows.n : (R + 1) + R * (2 * R + 1);
   const uint32_t pitch = cellOffPitch((uint32_t)nx);
   __syncwarp();
-  for (int q0 = 0; q0 < nq; q0 += kWalkGroup) {
-    const int gq = min(kWalkGroup, nq - q0);  // warp-uniform
-    uint32_t lo[kWalkGroup], cnt[kWalkGroup];
+  for (int q0 = 0; q0 < nq; q0 += G) {
+    const int gq = R1 ? G : min(G, nq - q0);  // warp-uniform
+    uint32_t lo[G], cnt[G];
 #pragma unroll
-    for (int t = 0; t < kWalkGroup; ++t) {
+    for (int t = 0; t < G; ++t) {
       lo[t] = 0u;
       cnt[t] = 0u;
       if (t >= gq) continue;
       int dz, dy, w;
-      halfRow(rows, q0 + t, R, c2, reachR2, dz, dy, w);
+      if constexpr (R1) {
+        dz = t >= 2 ? 1 : 0;
+        dy = t == 0 ? 0 : t == 1 ? 1 : t - 3;
+        w = 1;
+      } else {
+        halfRow(rows, q0 + t, R, c2, reachR2, dz, dy, w);
+      }
       const bool own = dz == 0 && dy == 0;
       const int32_t jz = iz + dz, jy = iy + dy;
       int32_t lo32 = own ? ix : max(ix - w, 0), hi32 = min(ix + w, nx - 1);
@@ -404,7 +414,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
     // item prefix and window rank of every lane (two warp scans in one)
     uint32_t tot = 0, nonEmpty = 0;
 #pragma unroll
-    for (int t = 0; t < kWalkGroup; ++t) {
+    for (int t = 0; t < G; ++t) {
       tot += cnt[t];
       nonEmpty += cnt[t] ? 1u : 0u;
     }
@@ -423,7 +433,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
     {
       uint32_t item = inclT - tot, rank = inclE - nonEmpty;
 #pragma unroll
-      for (int t = 0; t < kWalkGroup; ++t) {
+      for (int t = 0; t < G; ++t) {
         if (cnt[t]) {
           sWin[warp][rank] = make_uint2(lo[t] - item, (uint32_t)lane);
           ++rank;
@@ -437,7 +447,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
       // windows started before the pass; marks of the windows starting inside it
       uint32_t before = 0, item = inclT - tot;
 #pragma unroll
-      for (int t = 0; t < kWalkGroup; ++t) {
+      for (int t = 0; t < G; ++t) {
         if (cnt[t]) {
           if (item < pass) ++before;
         }
@@ -446,7 +456,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
       __syncwarp();
       item = inclT - tot;
 #pragma unroll
-      for (int t = 0; t < kWalkGroup; ++t) {
+      for (int t = 0; t < G; ++t) {
         if (cnt[t] && item >= pass && item - pass < kDealPass)
           atomicOr(&sMask[warp][(item - pass) >> 5], 1u << ((item - pass) & 31u));
         item += cnt[t];

@@ -228,9 +228,9 @@ def test_adjoint_directional_fd_at_benchmark_size(capi):
     rel, counts = bench.fd_classify(np.sum(dx * d, axis=1), miss0, miss.reshape(k, n), step0,
                                     step.reshape(k, n), eps)
     resolved = np.isfinite(rel)
-    assert np.mean(resolved) > 0.95, counts  # some side of the stencil keeps the argmin step
+    assert np.mean(resolved) > 0.9, counts  # some side of the stencil keeps the argmin step and is smooth
     assert np.median(rel[resolved]) < 1e-7, np.median(rel[resolved])
-    assert np.mean(rel[resolved] <= 1e-6) > 0.99, (counts, np.sort(rel[resolved])[-10:])
+    assert np.mean(rel[resolved] <= 1e-6) > 0.98, (counts, np.sort(rel[resolved])[-10:])
 
 
 @pytest.mark.gpu
