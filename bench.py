@@ -522,9 +522,50 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
             applied = {"iteration": first[0], "breakups": nb, "fragments_appended": nf, "objects_before": n0,
                        "objects_after": ctx.size(), "append_ms": t_append * 1e3,
                        "propagated_one_step": True, "nonfinite_after_step": not ok, "escaped_after_step": gone}
-    return {"iterations": iterations, "hours": iterations * cfg.deltaT / 3600.0, **tot,
-            "expected_collisions_from_conjunctions": expected, "first_breakup_applied": applied,
-            "ms_per_iteration_wall": wall * 1e3 / iterations}
+    out = {"iterations": iterations, "hours": iterations * cfg.deltaT / 3600.0, **tot,
+           "expected_collisions_from_conjunctions": expected, "first_breakup_applied": applied,
+           "ms_per_iteration_wall": wall * 1e3 / iterations}
+    out["applied_run"] = applied_breakup_run(capi, cfg, bcfg, pop, iterations, min_altitude)
+    return out
+
+
+def applied_breakup_run(capi, cfg, bcfg, pop, iterations, min_altitude, wall_budget_s=45.0):
+    """The same loop with every breakup applied: fragments appended on the
+    device (ladds_gpu_breakup), burn-ups and escaping fragments removed, until
+    the day ends, the wall budget is spent or a call fails.  Fragments of one
+    breakup start at one point; their same-parent pairs are skipped by the
+    functor (spawn protection) but still visited by the cell scan, so a large
+    breakup slows the following iterations until the cloud disperses."""
+    n = len(pop["x"])
+    next_id = int(np.max(pop["id"])) + 1 if n else 0
+    tot = dict(iterations=0, breakups=0, fragments=0, burnups=0, escaped=0)
+    times = []
+    err = None
+    t0 = time.perf_counter()
+    with capi.Context(cfg) as ctx:
+        ctx.upload(pop)
+        try:
+            for it in range(iterations):
+                t1 = time.perf_counter()
+                ctx.integrate(1, allow_nonfinite=True)
+                tot["burnups"] += len(ctx.remove_below(min_altitude))
+                tot["escaped"] += len(ctx.remove_escaping())
+                rec = ctx.conjunctions(cfg.deltaT)
+                if np.any(rec["flags"] & capi.PAIR_COLLISION):
+                    nb, nf, next_id = ctx.breakup(rec, bcfg, 1000 + it, next_id)
+                    tot["breakups"] += nb
+                    tot["fragments"] += nf
+                tot["iterations"] = it + 1
+                times.append(time.perf_counter() - t1)
+                if time.perf_counter() - t0 > wall_budget_s:
+                    break
+        except Exception as ex:  # noqa: BLE001
+            err = str(ex)[:160]
+        size = ctx.size()
+    last = times[-100:] if times else [0.0]
+    return {**tot, "objects_after": size, "stopped_by": "error" if err else
+            ("wall budget" if tot["iterations"] < iterations else "end of run"), "error": err,
+            "ms_per_iteration_last_100": float(np.mean(last)) * 1e3, "wall_budget_s": wall_budget_s}
 
 
 # ---------------------------------------------------------- adjoint leg
@@ -877,8 +918,10 @@ def main():
                   for k, v in drift.items()},
         "adjoint_over_forward": (adjoint or {}).get("backward_over_forward"),
         "adjoint_fd": (adjoint or {}).get("fd_summary"),
-        "breakups_8e6": ({k: breakups[k] for k in ("iterations", "collisions", "breakups", "fragments", "burnups",
-                                                    "escaped", "expected_collisions_from_conjunctions")}
+        "breakups_8e6": ({**{k: breakups[k] for k in ("iterations", "collisions", "breakups", "fragments",
+                                                       "expected_collisions_from_conjunctions")},
+                          "applied": {k: breakups["applied_run"][k] for k in ("iterations", "breakups", "fragments",
+                                                                              "stopped_by")}}
                          if breakups and "error" not in breakups else breakups),
         "value_over_cpu_baseline": value / cpu["value"] if cpu and cpu.get("value") else None,
     }

@@ -34,17 +34,28 @@ constexpr int kBucketThreads = 256;
 // Occupancy bin of the pair scan: cells holding at least minCount objects are
 // listed (key r * nx + ix) by the row sorts; their objects are scanned by cell
 // tiles (k_pair_tiles) instead of the per-object walk.  cells == nullptr: off.
+// A cell of more than kTileChunk objects is listed once per chunk of
+// kTileChunk source objects (cells[q], chunk[q] = chunk index), so that the
+// objects of a crowded cell -- a breakup's fragments start at one point -- are
+// shared out over many warps.
 struct DenseBin {
   uint32_t *cells;
   uint32_t *count;
   uint32_t cap;
   uint32_t minCount;
+  uint32_t *chunk;
 };
-constexpr uint32_t kDenseCell = 12;  // objects per cell from which the cell is scanned by tiles
+constexpr uint32_t kDenseCell = 12;   // objects per cell from which the cell is scanned by tiles
+constexpr uint32_t kTileChunk = 256;  // source objects of one dense-bin work item
 
-__device__ __forceinline__ void denseAppend(const DenseBin &d, uint32_t key) {
-  const uint32_t q = atomicAdd(d.count, 1u);
-  if (q < d.cap) d.cells[q] = key;
+__device__ __forceinline__ void denseAppend(const DenseBin &d, uint32_t key, uint32_t objects) {
+  const uint32_t nch = (objects + kTileChunk - 1) / kTileChunk;
+  const uint32_t q = atomicAdd(d.count, nch);
+  for (uint32_t ch = 0; ch < nch; ++ch)
+    if (q + ch < d.cap) {
+      d.cells[q + ch] = key;
+      d.chunk[q + ch] = ch;
+    }
 }
 
 __device__ __forceinline__ uint32_t laneMaskLt() {
@@ -343,7 +354,7 @@ __device__ __forceinline__ void sortOneRow(uint32_t r, uint32_t s0, uint32_t L, 
         v[i] = run;
         run0[i] = run;
         run += c;
-        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * 8u + i);
+        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * 8u + i, c);
       }
       *reinterpret_cast<uint4 *>(cellOff + (size_t)r * pitch + lane * 8u) =
           make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
@@ -353,7 +364,7 @@ __device__ __forceinline__ void sortOneRow(uint32_t r, uint32_t s0, uint32_t L, 
         const uint32_t c = run0[i];
         run0[i] = run;
         run += c;
-        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * per + i);  // counts past nx are 0
+        if (listDense && c >= dense.minCount) denseAppend(dense, r * nx + lane * per + i, c);  // counts past nx are 0
       }
       __syncwarp();
       if (cellOff) {
@@ -498,8 +509,26 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
       fillCellOffsets(t, nx, L, [&](uint32_t i) { return (uint32_t)(V[i] >> 32); }, threadIdx.x, blockDim.x);
       __syncthreads();
       if (dense.cells)
-        for (uint32_t c = threadIdx.x; c < nx; c += blockDim.x)
-          if ((uint32_t)(t[c + 1] - t[c]) >= dense.minCount) denseAppend(dense, r * nx + c);
+        for (uint32_t c = threadIdx.x; c < nx; c += blockDim.x) {
+          const uint32_t m = (uint32_t)(t[c + 1] - t[c]);
+          if (m >= dense.minCount) denseAppend(dense, r * nx + c, m);
+        }
+    } else if (dense.cells) {
+      // a row too long for 16-bit offsets: its crowded cells are found from the
+      // sorted records (each cell's first record searches for the cell's end)
+      for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+        const uint32_t ix = (uint32_t)(V[i] >> 32);
+        if (i > 0 && (uint32_t)(V[i - 1] >> 32) == ix) continue;
+        uint32_t a = i + 1, b = L;
+        while (a < b) {
+          const uint32_t mid = (a + b) >> 1;
+          if ((uint32_t)(V[mid] >> 32) <= ix)
+            a = mid + 1;
+          else
+            b = mid;
+        }
+        if (a - i >= dense.minCount) denseAppend(dense, r * nx + ix, a - i);
+      }
     }
     __syncthreads();
   }

@@ -33,11 +33,22 @@ __device__ __forceinline__ float4 floatPosition(double x, double y, double z) {
 // in cell order, and, for the few pairs that reach the binary64 functor, the
 // state as it was before the gather (src, indexed through perm) -- the next
 // propagation, which runs beside the scan, writes only the gathered copy.
+// Breakup group of an object in the scan: its parent id when that fits 32
+// bits, else kNoGroup (no parent, or an id too large to compare here: such
+// pairs are left to the functor's own parent test).  Two objects of one group
+// cannot yield a record (CollisionFunctor.cpp:64-67), so the pair scan skips
+// them before they become candidates.
+constexpr uint32_t kNoGroup = 0xffffffffu;
+__device__ __forceinline__ uint32_t groupOf(uint64_t parent) {
+  return parent < (uint64_t)kNoGroup ? (uint32_t)parent : kNoGroup;
+}
+
 struct ScanPack {
   float4 *posf;          // binary32 x, y, z + rounding bound
   float4 *velf;          // binary32 vx, vy, vz + radius rounded up
   DevState src;          // state before the gather
   const uint32_t *perm;  // cell-order position -> index in src
+  uint32_t *grp;         // breakup group per cell-order position (null: no object has a parent)
 };
 
 __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict__ perm, int n, ScanPack pk,
@@ -53,6 +64,7 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
   const double vx = src.vx[p], vy = src.vy[p], vz = src.vz[p];
   const uint32_t tag = src.tag[p];
   const double radius = tagSlot(tag) < (uint32_t)n ? src.radius[tagSlot(tag)] : 0.0;  // slot-indexed
+  if (pk.grp) pk.grp[j] = tagSlot(tag) < (uint32_t)n ? groupOf(src.parent[tagSlot(tag)]) : kNoGroup;
   dst.x[j] = x;
   dst.y[j] = y;
   dst.z[j] = z;

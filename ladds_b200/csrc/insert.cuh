@@ -125,7 +125,8 @@ __global__ void k_selected_positions(const uint32_t *__restrict__ sel, const uin
 
 // State records (device memory) appended at positions / slots offset..offset+m
 // (slot-indexed radius, id and parent at the same index); bad[0] counts
-// records with a non-finite value or an activity state out of range.
+// records with a non-finite value or an activity state out of range, bad[1]
+// is set when a record has a parent id.
 __global__ void k_append_records(const ladds_state_record *__restrict__ in, int m, DevState s, uint32_t offset,
                                  unsigned *__restrict__ bad) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -136,6 +137,7 @@ __global__ void k_append_records(const ladds_state_record *__restrict__ in, int 
                   isfinite(r.v[1]) && isfinite(r.v[2]) && isfinite(r.radius) && isfinite(r.aom) &&
                   isfinite(r.bcInv) && r.activity >= 0 && r.activity <= 2;
   if (!ok) atomicAdd(bad, 1u);
+  if (r.parentId != UINT64_MAX) atomicOr(bad + 1, 1u);
   s.x[at] = r.r[0];
   s.y[at] = r.r[1];
   s.z[at] = r.r[2];

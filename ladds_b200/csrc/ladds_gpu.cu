@@ -95,6 +95,8 @@ struct ladds_gpu_ctx {
   uint32_t *scanWs = nullptr;             // block sums of the exclusive scans
   float4 *posf = nullptr;                 // binary32 positions + rounding bound, cell order
   float4 *velf = nullptr;                 // binary32 velocities + radius of the cell order
+  uint32_t *grp = nullptr;                // breakup group of the cell order (parent id, or kNoGroup)
+  bool anyParent = false;                 // some object has a parent id: the scan writes and reads grp
   uint32_t *rowStart = nullptr;
   uint32_t nRows = 0;
   uint32_t *scratchA = nullptr, *scratchB = nullptr, *scratchC = nullptr, *blockSums = nullptr;
@@ -124,6 +126,7 @@ struct ladds_gpu_ctx {
   float cutF = 0.f;         // binary32 pre-filter radius: cutoff * (1 + nearRel), rounded up
   int chunkSteps = kMaxEphSteps;  // iterations per ephemeris chunk / captured graph (autotuned)
   uint32_t *denseCells = nullptr, *denseCount = nullptr;  // dense bin of the pair scan (cells >= kDenseCell)
+  uint32_t *denseChunk = nullptr, *denseChunkB = nullptr;  // chunk index of each dense-bin entry
   uint32_t haloStart = 0xffffffffu;  // objects with slot >= haloStart: pair-scan targets only
   uint32_t denseCap = 0;
   // second set of the sort results: the sort of a step writes one set while the
@@ -236,11 +239,12 @@ void freeBuffers(ladds_gpu_ctx *c) {
   freeState(c->alt, false);
   freeState(c->snap, false);
   void *ptrs[] = {c->keys0, c->keys1, c->vals0, c->vals1, c->scratchA, c->scratchB, c->scratchC,
-                  c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf, c->keys1B, c->vals1B};
+                  c->blockSums, c->posf, c->sortRec, c->scanWs, c->velf, c->keys1B, c->vals1B, c->grp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   c->posf = nullptr;
   c->velf = nullptr;
+  c->grp = nullptr;
   c->sortRec = nullptr;
   c->scanWs = nullptr;
   c->keys0 = c->keys1 = c->vals0 = c->vals1 = c->keys1B = c->vals1B = nullptr;
@@ -291,23 +295,29 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
   const size_t wsWords = 4 * (scanLen / kScanBlock + 2) + 4 * kScanBlock;
   if (cudaMalloc(&c->posf, newCap * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&c->velf, newCap * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&c->grp, newCap * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->sortRec, newCap * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->scanWs, wsWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->blockSums, (scanBlocks + 1) * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
     return fail(c, LADDS_ERR_ALLOC, "device allocation failed (cell-order buffers)");
   }
-  if (c->denseCells) cudaFree(c->denseCells);
-  if (c->denseCellsB) cudaFree(c->denseCellsB);
-  c->denseCells = c->denseCellsB = nullptr;
-  c->denseCap = (uint32_t)(newCap / kDenseCell + 1);
-  if (cudaMalloc(&c->denseCells, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&c->denseCellsB, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
-    cudaGetLastError();
-    if (c->denseCells) cudaFree(c->denseCells);
-    c->denseCells = c->denseCellsB = nullptr;
-    c->denseCap = 0;
-    return fail(c, LADDS_ERR_ALLOC, "device allocation failed (dense-cell list)");
+  for (uint32_t **p : {&c->denseCells, &c->denseCellsB, &c->denseChunk, &c->denseChunkB}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  // every listed cell holds >= kDenseCell objects and adds one entry per kTileChunk of them
+  c->denseCap = (uint32_t)(newCap / kDenseCell + newCap / kTileChunk + 1);
+  for (uint32_t **p : {&c->denseCells, &c->denseCellsB, &c->denseChunk, &c->denseChunkB}) {
+    if (cudaMalloc(p, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      for (uint32_t **q : {&c->denseCells, &c->denseCellsB, &c->denseChunk, &c->denseChunkB}) {
+        if (*q) cudaFree(*q);
+        *q = nullptr;
+      }
+      c->denseCap = 0;
+      return fail(c, LADDS_ERR_ALLOC, "device allocation failed (dense-cell list)");
+    }
   }
   c->cap = newCap;
   c->orderValid = false;
@@ -515,7 +525,7 @@ void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, ui
 DenseBin denseBin(const ladds_gpu_ctx *c) {
   const bool on = c->cellOff && c->denseCells && (uint32_t)c->grid.n[0] <= (uint32_t)kRowCountMaxNx &&
                   c->grid.reach <= 3;  // k_pair_tiles: one lane per half-shell row (<= 25 rows)
-  return DenseBin{on ? c->denseCells : nullptr, c->denseCount, c->denseCap, kDenseCell};
+  return DenseBin{on ? c->denseCells : nullptr, c->denseCount, c->denseCap, kDenseCell, c->denseChunk};
 }
 
 // the sort writes the result set that the previous pair scan does not read
@@ -525,6 +535,7 @@ void swapSortSets(ladds_gpu_ctx *c) {
   std::swap(c->vals1, c->vals1B);
   std::swap(c->cellOff, c->cellOffB);
   std::swap(c->denseCells, c->denseCellsB);
+  std::swap(c->denseChunk, c->denseChunkB);
   std::swap(c->denseCount, c->denseCountB);
   c->sortParity ^= 1;
 }
@@ -565,7 +576,9 @@ void enqueueSort(ladds_gpu_ctx *c) {
 }
 
 // after the gather (enqueueCells) alt holds the state as the scan sees it, perm maps into it
-inline ScanPack scanPack(ladds_gpu_ctx *c) { return ScanPack{c->posf, c->velf, c->alt, c->perm}; }
+inline ScanPack scanPack(ladds_gpu_ctx *c) {
+  return ScanPack{c->posf, c->velf, c->alt, c->perm, c->anyParent ? c->grp : nullptr};
+}
 
 // gathers the state into cell order (so that the next propagation, key pass and
 // gather read nearly sequentially: objects move about one cell per step) and
@@ -589,7 +602,8 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
   {
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
     cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
-    const CandSink out{sc, c->posf, c->velf, c->dCand, c->dCandCount, (unsigned long long)c->candCap, c->haloStart};
+    const CandSink out{sc,       c->posf,     c->velf,      c->dCand, c->dCandCount, (unsigned long long)c->candCap,
+                       c->haloStart, c->anyParent ? c->grp : nullptr};
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
     // the largest separation a record or a near-band flag can have, with room for rounding
     const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
@@ -607,8 +621,8 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
               : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(
-          dense.cells, dense.count, dense.cap, c->cur.tag, c->posf, c->sortedKeys, c->rowStart, c->cellOff, c->grid,
-          cutF, reach * reach, out);
+          dense.cells, dense.chunk, dense.count, dense.cap, c->cur.tag, c->posf, c->sortedKeys, c->rowStart,
+          c->cellOff, c->grid, cutF, reach * reach, out);
   }
   PhaseScope ps(c, kPhEvaluate, s);
   const int b = c->cfg.scanBlock > 0 ? c->cfg.scanBlock : 256;
@@ -737,6 +751,7 @@ int writeArrays(ladds_gpu_ctx *c, size_t offset, size_t n, const double *x, cons
   CK(cudaMemcpyAsync(c->cur.id + offset, id, n * sizeof(uint64_t), cudaMemcpyHostToDevice, c->st));
   std::vector<uint64_t> par;
   if (!parentId) par.assign(n, UINT64_MAX);
+  for (size_t i = 0; i < n && parentId && !c->anyParent; ++i) c->anyParent = parentId[i] != UINT64_MAX;
   CK(cudaMemcpyAsync(c->cur.parent + offset, parentId ? parentId : par.data(), n * sizeof(uint64_t),
                      cudaMemcpyHostToDevice, c->st));
   std::vector<uint32_t> tags(n);
@@ -945,7 +960,7 @@ int ladds_gpu_destroy(ladds_gpu_ctx *c) {
   freeBuffers(c);
   freeGridBuffers(c);
   void *ptrs[] = {c->longCount, c->denseCount, c->denseCells, c->denseCountB, c->denseCellsB, c->dCount,
-                  c->dEph,
+                  c->denseChunk, c->denseChunkB, c->dEph,
                   c->dIter, c->dPairs, c->dCand, c->dCandCount, c->dObj,
                   c->adj.st, c->adj.bc, c->adj.aom, c->adj.miss, c->adj.grad, c->adj.ckpt, c->adj.rec,
                   c->adj.off, c->adj.arg, c->adj.eph};
@@ -985,6 +1000,7 @@ int ladds_gpu_upload(ladds_gpu_ctx *c, size_t n, const double *x, const double *
   rc = ensureCapacity(c, n);
   if (rc) return rc;
   c->n = 0;
+  c->anyParent = false;
   rc = writeArrays(c, 0, n, x, y, z, vx, vy, vz, radius, aom, bcInv, id, parentId, activity);
   if (rc) return rc;
   c->n = n;
@@ -1939,14 +1955,16 @@ int ladds_gpu_append_records(ladds_gpu_ctx *c, const ladds_state_record *records
   if (c->n + m > (size_t)kTagSlotMask) return fail(c, LADDS_ERR_TOO_LARGE, "append_records: too many particles");
   int rc = ensureCapacity(c, c->n + m);
   if (rc) return rc;
-  unsigned *dBad = reinterpret_cast<unsigned *>(c->dCandNeed);  // scratch word (reset by every scan)
-  CK(cudaMemsetAsync(dBad, 0, sizeof(unsigned), c->st));
+  // scratch words (reset by every scan): [0] bad records, [1] records with a parent
+  unsigned *dBad = reinterpret_cast<unsigned *>(c->dCandNeed);
+  CK(cudaMemsetAsync(dBad, 0, 2 * sizeof(unsigned), c->st));
   k_append_records<<<blocksFor(m, 128), 128, 0, c->st>>>(records, (int)m, c->cur, (uint32_t)c->n, dBad);
   CK(cudaGetLastError());
-  unsigned bad = 0;
-  CK(cudaMemcpyAsync(&bad, dBad, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  unsigned flags[2] = {0, 0};
+  CK(cudaMemcpyAsync(flags, dBad, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  if (bad) return fail(c, LADDS_ERR_INVALID_ARG, "append_records: a record holds NaN/Inf or a bad activity state");
+  if (flags[0]) return fail(c, LADDS_ERR_INVALID_ARG, "append_records: a record holds NaN/Inf or a bad activity state");
+  if (flags[1]) c->anyParent = true;
   c->n += m;
   c->orderValid = false;
   dropGraphs(c);
@@ -2692,7 +2710,7 @@ int ladds_gpu_cell_sort_noalloc(int device, void *stream, const uint32_t *keys, 
     if (ok(cudaGetLastError())) {
       k_bucket_sort_large<<<2 * d.sms, kBucketThreads, kLargeRow * 12, s>>>(
           rowStartS, nx, rec, src, sortedKeys, order, longRows, longCount, nullptr,
-          DenseBin{nullptr, nullptr, 0, 0});
+          DenseBin{nullptr, nullptr, 0, 0, nullptr});
       ok(cudaGetLastError());
     }
   }

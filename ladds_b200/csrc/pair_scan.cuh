@@ -132,6 +132,7 @@ struct CandSink {
   unsigned long long *count;
   unsigned long long half;
   uint32_t haloStart;  // objects with slot >= haloStart are scan targets only, never sources
+  const uint32_t *grp;  // breakup group per cell-order position (null: no object has a parent)
 };
 
 // Per-warp candidate buffer in shared memory with its fill count n held in a
@@ -314,6 +315,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
   __shared__ uint2 sWin[W][32 * G];  // (lo - first item, owner lane) by window rank
   __shared__ uint32_t sMask[W][kDealPass / 32];
   __shared__ float4 sOwn[W][32];
+  __shared__ uint32_t sGrp[W][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
   const int warpBase = blockIdx.x * kScanCta + warp * 32;
@@ -331,15 +333,14 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
     iz = (int32_t)(row / (uint32_t)ny);
     // objects of the dense bin (own cell >= denseMin objects) are scanned by k_pair_tiles
     if (cellOff && denseMin != 0xffffffffu && __ldg(denseCount) != 0u) {
-      const uint32_t rs0 = __ldg(&rowStart[row]), rs1 = __ldg(&rowStart[row + 1]);
-      if (rs1 - rs0 <= 65535u) {
-        const uint16_t *t = cellOff + (size_t)row * cellOffPitch((uint32_t)nx);
-        if ((uint32_t)(__ldg(&t[ix + 1]) - __ldg(&t[ix])) >= denseMin) active = false;
-      }
+      uint32_t a, b;  // the own cell's objects (rows beyond 16-bit offsets: searched)
+      rowWindow(row, (uint32_t)ix, (uint32_t)ix, (uint32_t)nx, rowStart, cellOff, skeys, a, b);
+      if (b - a >= denseMin) active = false;
     }
   }
   const float4 me = inRange ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
   sOwn[warp][lane] = me;
+  if (out.grp) sGrp[warp][lane] = inRange ? __ldg(&out.grp[j]) : kNoGroup;
   const double c2 = g.cellSize * g.cellSize;
   // Dense populations (the buffer form) with cells below the cutoff (reach >=
   // 2): the object's own x-window in each neighbour row: partners lie within
@@ -477,6 +478,10 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
           k = wv.x + it;
           jj = (uint32_t)warpBase + wv.y;
           pass2 = prefilterPass(sOwn[warp][wv.y], __ldg(&posf[k]), cutF);
+          if (pass2 && out.grp) {  // fragments of one breakup never yield a record
+            const uint32_t g = sGrp[warp][wv.y];
+            pass2 = g == kNoGroup || g != __ldg(&out.grp[k]);
+          }
         }
         warpAppend<SCREEN>(pass2, jj, k, lane, sCand[warp], nBuf, out);
       }
@@ -487,19 +492,24 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
 }
 
 // Dense bin of the pair scan (cells with >= kDenseCell objects, listed by the
-// row sorts): one warp per listed cell.  Lane q locates the window of
-// half-shell row q (the own row from the cell on; rows (dz, dy) > (0, 0) over
-// ix - R .. ix + R) -- all rows' lookups in flight together -- and the warp
-// stages up to kTileStage neighbour objects of the concatenated windows in
-// shared memory with independent loads.  Then every source lane (the cell's
-// objects, 32 at a time) tests every staged object: no per-pair address work,
-// no divergence but the survivors', no dependent global load inside the loop.
-// Own-row objects are paired with later objects only.  Same pre-filter and
-// candidate output as k_pair_candidates, which skips these objects as sources.
+// row sorts, one entry per kTileChunk of their objects): one warp per entry.
+// Lane q locates the window of half-shell row q (the own row from the cell on;
+// rows (dz, dy) > (0, 0) over ix - R .. ix + R) -- all rows' lookups in flight
+// together -- and the warp stages up to kTileStage neighbour objects of the
+// concatenated windows in shared memory with independent loads.  Then every
+// source lane (the entry's chunk of the cell's objects, 32 at a time) tests
+// every staged object: no per-pair address work, no divergence but the
+// survivors', no dependent global load inside the loop.  Own-row objects are
+// paired with later objects only.  Pairs of one breakup group are skipped: a
+// staged block and a source batch that both belong to one group entirely are
+// not tested at all (a breakup's fragments start at one point, in one cell).
+// Same pre-filter and candidate output as k_pair_candidates, which skips these
+// objects as sources.
 constexpr uint32_t kTileStage = 256;  // staged neighbour objects per warp and pass
 
 template <int SCREEN>
 __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restrict__ denseCells,
+                                                         const uint32_t *__restrict__ denseChunk,
                                                          const uint32_t *__restrict__ denseCount, uint32_t denseCap,
                                                          const uint32_t *__restrict__ tags,
                                                          const float4 *__restrict__ posf,
@@ -510,21 +520,22 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
   __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
   __shared__ float4 sNb[kScanCta / 32][kTileStage];
   __shared__ uint32_t sK[kScanCta / 32][kTileStage];
+  __shared__ uint32_t sG[kScanCta / 32][kTileStage];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
   const uint32_t nDense = min(*denseCount, denseCap);
   const uint32_t gw = (blockIdx.x * kScanCta + threadIdx.x) >> 5, nW = (gridDim.x * kScanCta) >> 5;
   const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
   const int nq = (R + 1) + R * (2 * R + 1);  // half-shell rows (<= 32 for R <= 3)
-  const uint32_t pitch = cellOffPitch((uint32_t)nx);
+  const uint32_t *grp = out.grp;
   for (uint32_t q = gw; q < nDense; q += nW) {
     const uint32_t key = denseCells[q];
     const uint32_t r = key / (uint32_t)nx;
     const int32_t ix = (int32_t)(key - r * (uint32_t)nx), iy = (int32_t)(r % (uint32_t)ny),
                   iz = (int32_t)(r / (uint32_t)ny);
-    const uint32_t rs = __ldg(&rowStart[r]);
-    const uint16_t *t = cellOff + (size_t)r * pitch;
-    const uint32_t c0 = rs + __ldg(&t[ix]), c1 = rs + __ldg(&t[ix + 1]);
+    uint32_t c0, c1;  // the cell's objects
+    rowWindow(r, (uint32_t)ix, (uint32_t)ix, (uint32_t)nx, rowStart, cellOff, skeys, c0, c1);
+    const uint32_t s0 = c0 + denseChunk[q] * kTileChunk, s1 = min(c1, s0 + kTileChunk);  // this entry's sources
     // lane q: window of half-shell row q
     uint32_t lo = 0, hi = 0;
     if (lane < nq) {
@@ -532,16 +543,11 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
       halfShellRowOf(lane, R, dz, dy);
       const int32_t jz = iz + dz, jy = iy + dy;
       const int w = rowHalfWidth(dy, dz, R, g.cellSize * g.cellSize, reachR2);
-      const uint32_t xlo = (uint32_t)max(ix - w, 0), xhi = (uint32_t)min(ix + w, nx - 1);
-      if (w >= 0 && jz < nz && jy >= 0 && jy < ny) {
-        if (lane == 0) {
-          lo = c0;
-          hi = rs + __ldg(&t[xhi + 1]);
-        } else {
-          rowWindow((uint32_t)jz * (uint32_t)ny + (uint32_t)jy, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys,
-                    lo, hi);
-        }
-      }
+      const uint32_t xlo = lane == 0 ? (uint32_t)ix : (uint32_t)max(ix - w, 0);
+      const uint32_t xhi = (uint32_t)min(ix + w, nx - 1);
+      if (w >= 0 && jz < nz && jy >= 0 && jy < ny)
+        rowWindow((uint32_t)jz * (uint32_t)ny + (uint32_t)jy, xlo, xhi, (uint32_t)nx, rowStart, cellOff, skeys, lo,
+                  hi);
     }
     const uint32_t cnt = hi - lo;
     uint32_t incl = cnt;
@@ -555,26 +561,41 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
     const uint32_t ownEnd = __shfl_sync(0xffffffffu, incl, 0);  // staged items [0, ownEnd) are own-row objects
     for (uint32_t stBase = 0; stBase < total; stBase += kTileStage) {
       const uint32_t m = min(kTileStage, total - stBase);
+      bool oneGroup = grp != nullptr;  // every staged object in one breakup group (warp-uniform after the loop)
+      uint32_t g0 = kNoGroup;
       for (uint32_t ib = 0; ib < m; ib += 32u) {  // stage items stBase + i (warp-uniform loop)
         const uint32_t i = ib + (uint32_t)lane, item = stBase + i;
         // row of the item: the last lane whose excl <= item (empty rows share the next excl)
         const int owner = windowOwner(excl, item);
         const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
+        uint32_t gi = kNoGroup;
         if (i < m) {
           const uint32_t k = oLo + (item - oEx);
           sNb[warp][i] = __ldg(&posf[k]);
           sK[warp][i] = k;
+          if (grp) {
+            gi = __ldg(&grp[k]);
+            sG[warp][i] = gi;
+          }
+        }
+        if (grp) {
+          if (ib == 0) g0 = __shfl_sync(0xffffffffu, gi, 0);
+          oneGroup = oneGroup && __all_sync(0xffffffffu, i >= m || (gi == g0 && gi != kNoGroup));
         }
       }
       __syncwarp();
-      for (uint32_t sBase = c0; sBase < c1; sBase += 32u) {
+      for (uint32_t sBase = s0; sBase < s1; sBase += 32u) {
         const uint32_t si = sBase + (uint32_t)lane;
-        const bool src = si < c1 && !tagDummy(tags[si]) && tagSlot(tags[si]) < out.haloStart;
+        const bool src = si < s1 && !tagDummy(tags[si]) && tagSlot(tags[si]) < out.haloStart;
+        const uint32_t gs = grp && si < s1 ? __ldg(&grp[si]) : kNoGroup;
+        // the batch and the staged block all in the same group: no pair can yield a record
+        if (oneGroup && __all_sync(0xffffffffu, !src || gs == g0)) continue;
         const float4 mf = src ? __ldg(&posf[si]) : make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t u = 0; u < m; ++u) {  // warp-uniform
           const float4 qq = sNb[warp][u];
           const uint32_t k = sK[warp][u];
-          const bool pass = src && prefilterPass(mf, qq, cutF) &&
+          const bool sameGroup = grp && gs != kNoGroup && gs == sG[warp][u];
+          const bool pass = src && !sameGroup && prefilterPass(mf, qq, cutF) &&
                             !(stBase + u < ownEnd && k <= si);  // own row: later objects only
           warpAppend<SCREEN>(pass, si, k, lane, sCand[warp], nBuf, out);
         }

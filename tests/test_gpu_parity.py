@@ -371,6 +371,53 @@ def test_nonfinite_state_is_reported_and_rolled_back(capi):
         assert np.array_equal(back["x"], pop["x"]) and ctx.iteration() == 0
 
 
+def fragment_clouds(seed):
+    """A dense population plus two breakup clouds 10 km apart: 3000 fragments
+    of parent 4242 within 0.5 km of one point (one cell, many dense-bin
+    chunks), 1000 of parent 5151 around a second point, and 20 objects with a
+    parent id beyond 32 bits inside the first cloud (left to the functor's own
+    parent test)."""
+    rng = np.random.default_rng(seed)
+    base = dense_population(seed, n=3000)
+    parts = [base]
+    for centre, count, parent in (((7050.0, 30.0, -20.0), 3000, 4242), ((7060.0, 30.0, -20.0), 1000, 5151),
+                                  ((7050.0, 30.0, -20.0), 20, 1 << 40)):
+        r = np.array(centre) + rng.uniform(-0.5, 0.5, size=(count, 3))
+        v = np.array([0.0, 7.5, 0.0]) + rng.normal(scale=0.05, size=(count, 3))
+        radius = np.exp(rng.uniform(np.log(0.01), np.log(0.2), count))
+        mass = 2700 * 4 / 3 * np.pi * radius ** 3
+        parts.append(dict(x=r[:, 0], y=r[:, 1], z=r[:, 2], vx=v[:, 0], vy=v[:, 1], vz=v[:, 2], radius=radius,
+                          aom=np.pi * radius ** 2 * 1e-6 / mass, bc_inv=2.2 * np.pi * radius ** 2 / mass,
+                          id=np.zeros(count, np.uint64), parent=np.full(count, np.uint64(parent)),
+                          activity=np.zeros(count, np.int8)))
+    pop = {k: np.concatenate([p_[k] for p_ in parts]) for k in base}
+    pop["id"] = np.arange(len(pop["x"]), dtype=np.uint64) + 10
+    return pop
+
+
+@pytest.mark.parametrize("screen", [0, 1])
+@pytest.mark.parametrize("cell", [0.0, 7.0])
+def test_breakup_clouds_bitexact_vs_oracle(capi, oracle, cell, screen):
+    """Fragments of one breakup start at one point: their pairs are skipped
+    before they become candidates (whole blocks of one group in the dense-bin
+    tiles, single pairs in the walk), the crowded cell is shared out in
+    chunks, and the records still equal the oracle's, which skips them in the
+    functor (CollisionFunctor.cpp:64-67)."""
+    pop = fragment_clouds(31)
+    dt = 10.0
+    with ctx_for(capi, cellSize=cell, scanScreen=screen, **DENSE_KW) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(dt)
+    p = oracle.scan_params(cutoff=20.0, dt=dt, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
+                           conjunction_threshold=2.0)
+    opop = to_oracle(oracle, pop)
+    ref = oracle.scan_cells(opop, p, oracle.make_grid(DENSE_BOX[0], DENSE_BOX[1], cell, 20.0))
+    assert records_equal(ref, oracle.scan_bruteforce(opop, p, cap=len(ref) + 1024))
+    big = set(range(10 + 3000 + 4000, 10 + 3000 + 4020))  # the 32-bit-overflow parents: records with the cloud
+    assert sum(1 for r in ref if int(r["idA"]) in big or int(r["idB"]) in big) > 1000
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+
+
 def test_escaping_particles_leave_the_container(capi):
     """Simulation.cpp:314, :381-387: after an integration, particles outside
     the box and particles whose state became non-finite leave the container.
