@@ -618,7 +618,8 @@ def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3):
     rel[only_m] = err(bwd)[only_m]
     unresolved = ~keep_p & ~keep_m
     counts = {"central": int(agree.sum()), "ambiguous": int(kink.sum()), "forward_only": int(only_p.sum()),
-              "backward_only": int(only_m.sum()), "unresolved": int(unresolved.sum())}
+              "backward_only": int(only_m.sum()), "unresolved": int(unresolved.sum()),
+              "central_meeting_tol": int(np.sum(rel[agree] <= tol))}
     return rel, counts
 
 
