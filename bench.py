@@ -539,33 +539,48 @@ def applied_breakup_run(capi, cfg, bcfg, pop, iterations, min_altitude, wall_bud
     n = len(pop["x"])
     next_id = int(np.max(pop["id"])) + 1 if n else 0
     tot = dict(iterations=0, breakups=0, fragments=0, burnups=0, escaped=0)
-    times = []
+    parts = ("integrate", "burnups", "escaping", "scan", "breakups")
+    times = []  # per iteration: wall seconds of each part
     err = None
     t0 = time.perf_counter()
     with capi.Context(cfg) as ctx:
         ctx.upload(pop)
         try:
             for it in range(iterations):
-                t1 = time.perf_counter()
+                t = [time.perf_counter()]
                 ctx.integrate(1, allow_nonfinite=True)
+                t.append(time.perf_counter())
                 tot["burnups"] += len(ctx.remove_below(min_altitude))
+                t.append(time.perf_counter())
                 tot["escaped"] += len(ctx.remove_escaping())
+                t.append(time.perf_counter())
                 rec = ctx.conjunctions(cfg.deltaT)
+                t.append(time.perf_counter())
                 if np.any(rec["flags"] & capi.PAIR_COLLISION):
                     nb, nf, next_id = ctx.breakup(rec, bcfg, 1000 + it, next_id)
                     tot["breakups"] += nb
                     tot["fragments"] += nf
+                t.append(time.perf_counter())
                 tot["iterations"] = it + 1
-                times.append(time.perf_counter() - t1)
+                times.append(np.diff(t))
                 if time.perf_counter() - t0 > wall_budget_s:
                     break
+            if times:  # where the last iterations' time goes, on the device
+                ctx.set_profiling(True)
+                ctx.conjunctions(cfg.deltaT)
+                pt = ctx.phase_times()
+                device_scan = {p: round(getattr(pt, p + "Ms"), 3) for p in capi.PhaseTimes.PHASES}
+                ctx.set_profiling(False)
         except Exception as ex:  # noqa: BLE001
             err = str(ex)[:160]
         size = ctx.size()
-    last = times[-100:] if times else [0.0]
+    last = np.mean(times[-100:], axis=0) * 1e3 if times else np.zeros(len(parts))
     return {**tot, "objects_after": size, "stopped_by": "error" if err else
             ("wall budget" if tot["iterations"] < iterations else "end of run"), "error": err,
-            "ms_per_iteration_last_100": float(np.mean(last)) * 1e3, "wall_budget_s": wall_budget_s}
+            "ms_per_iteration_last_100": float(np.sum(last)),
+            "ms_last_100_by_part": {p: round(float(v), 3) for p, v in zip(parts, last)},
+            "device_ms_of_one_scan_at_the_end": device_scan if times and not err else None,
+            "wall_budget_s": wall_budget_s}
 
 
 # ---------------------------------------------------------- adjoint leg

@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
 }
 
 
-constexpr int kLargeRowThreads = 1024;  // threads of the long-row sort (rows beyond a warp's 256 objects)
+constexpr int kLargeRowThreads = 512;  // threads of the long-row sort (rows beyond a warp's 256 objects): two CTAs per SM
 __global__ void __launch_bounds__(kLargeRowThreads) k_bucket_sort_large(
     const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,
     uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,

@@ -569,7 +569,7 @@ void enqueueSort(ladds_gpu_ctx *c) {
     k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
         c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   }
-  k_bucket_sort_large<<<c->evalBlocks / 8, kLargeRowThreads, kLargeRow * 12, c->st>>>(
+  k_bucket_sort_large<<<c->evalBlocks / 2, kLargeRowThreads, kLargeRow * 12, c->st>>>(
       c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff, dense);
   c->sortedKeys = c->keys1;
   c->perm = c->vals1;
