@@ -772,7 +772,7 @@ def main():
     scale_kw = {}
     tuned = workloads.get("scale_8M", {}).get("autotuned")
     if tuned:
-        scale_kw = {k: tuned[k] for k in ("cellSize", "scanScreen", "propagateBlock", "scanBlock")}
+        scale_kw = {k: tuned[k] for k in ("cellSize", "scanScreen", "walkForm", "propagateBlock", "scanBlock")}
     if not args.no_drift and rank == 0:
         for name, mk_pop, steps, kw in (
                 ("population0_1e6", lambda: pop, STEPS_PER_DAY, {}),

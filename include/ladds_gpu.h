@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define LADDS_GPU_ABI_VERSION 2
+#define LADDS_GPU_ABI_VERSION 3
 
 /* ---- status codes ---- */
 #define LADDS_OK 0
@@ -113,6 +113,8 @@ typedef struct {
   uint64_t pairCapacity;          /* initial device pair-buffer capacity (0: auto)     */
   int32_t scanScreen;             /* LADDS_SCREEN_*: how the pair scan screens full
                                      candidate buffers (results do not depend on it)   */
+  int32_t walkForm;               /* LADDS_WALK_*: how the candidate walk deals its
+                                     items (results do not depend on it)               */
 } ladds_gpu_config;
 
 /* The binary32 closest-approach screen of the pre-filtered pairs (a superset
@@ -124,6 +126,14 @@ typedef struct {
  * pairs per object). */
 #define LADDS_SCREEN_LISTS 0
 #define LADDS_SCREEN_BUFFER 1
+/* The candidate walk deals each warp's neighbour-window items out 32 per round
+ * either over groups of up to eight rows at once (GROUPED: sparse populations,
+ * a few items per window) or row by row (ROWS: dense populations, many items
+ * per window).  AUTO: GROUPED for list screening with cells of reach 1, ROWS
+ * otherwise; the autotuner measures both. */
+#define LADDS_WALK_AUTO 0
+#define LADDS_WALK_GROUPED 1
+#define LADDS_WALK_ROWS 2
 
 typedef struct ladds_gpu_ctx ladds_gpu_ctx;
 
@@ -462,6 +472,8 @@ int ladds_records_write_csv(const char *path, int append, const ladds_pair *recs
  * traversal).  Times trials of the context's step on a copy of its population
  * (each trial: a fresh context, a warm-up call, then stepsPerTrial timed
  * iterations from the same start state) and applies the fastest to ctx:
+ *   0. screening form of full candidate buffers (LADDS_SCREEN_*) x walk form
+ *      (LADDS_WALK_GROUPED / _ROWS) at the current cell edge;
  *   1. cell edge: the current one, cutoff / R for reach R = 1..4 and 1.5 and 2
  *      cutoffs, those within [20, 160] km;
  *   2. propagateBlock x scanBlock in {128, 256}^2;
@@ -474,6 +486,7 @@ typedef struct {
   int32_t reach;            /* neighbour reach in cells */
   int32_t propagateBlock, scanBlock, chunkSteps;
   int32_t scanScreen;       /* LADDS_SCREEN_* */
+  int32_t walkForm;         /* LADDS_WALK_* */
   double msPerStep;         /* device time per iteration of the trial */
 } ladds_tune_trial;
 int ladds_gpu_autotune(ladds_gpu_ctx *ctx, int stepsPerTrial, ladds_tune_trial *trials, size_t cap, size_t *nTrials,

@@ -24,6 +24,7 @@ PROP_ALL = 0x1FF
 PASSIVE, EVASIVE, EVASIVE_PRESERVING = 0, 1, 2
 PRECISION_FP64, PRECISION_SPLIT = 0, 1
 SCREEN_LISTS, SCREEN_BUFFER = 0, 1
+WALK_AUTO, WALK_GROUPED, WALK_ROWS = 0, 1, 2
 PAIR_COLLISION, PAIR_EVASION, PAIR_CONJUNCTION = 1, 2, 4
 PAIR_NEAR_COLLISION, PAIR_NEAR_EVASION, PAIR_NEAR_CONJUNCTION, PAIR_NEAR_GATE = 8, 16, 32, 64
 SIZE_MAX = np.uint64(0xFFFFFFFFFFFFFFFF)
@@ -59,6 +60,7 @@ class GpuConfig(C.Structure):
         ("useGraphs", C.c_int32),
         ("pairCapacity", C.c_uint64),
         ("scanScreen", C.c_int32),
+        ("walkForm", C.c_int32),
     ]
 
 
@@ -115,7 +117,7 @@ assert OBJECT_DTYPE.itemsize == 80
 class TuneTrial(C.Structure):
     _fields_ = [("cellSize", C.c_double), ("reach", C.c_int32), ("propagateBlock", C.c_int32),
                 ("scanBlock", C.c_int32), ("chunkSteps", C.c_int32), ("scanScreen", C.c_int32),
-                ("msPerStep", C.c_double)]
+                ("walkForm", C.c_int32), ("msPerStep", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -457,8 +457,7 @@ __global__ void __launch_bounds__(kRowSortThreads) k_bucket_sort_rows(
 }
 
 
-constexpr int kLargeRowThreads = 512;  // threads of the long-row sort (rows beyond a warp's 256 objects): two CTAs per SM
-__global__ void __launch_bounds__(kLargeRowThreads) k_bucket_sort_large(
+__global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
     const uint32_t *__restrict__ rowStart, uint32_t nx, unsigned long long *__restrict__ rec,
     uint32_t *__restrict__ src, uint32_t *__restrict__ sortedKeys, uint32_t *__restrict__ perm,
     const uint32_t *__restrict__ longRows, const uint32_t *__restrict__ longCount,
@@ -482,36 +481,53 @@ __global__ void __launch_bounds__(kLargeRowThreads) k_bucket_sort_large(
       }
     }
     __syncthreads();
-    // the comparators of a stage touch disjoint pairs: each thread loads four
-    // pairs before it compares any, so that rows sorted in global memory (beyond
-    // kLargeRow objects: a breakup's fragment cloud) keep four loads in flight
     for (uint32_t k = 2; k <= P; k <<= 1) {
       for (uint32_t jj = k / 2; jj > 0; jj >>= 1) {
-        for (uint32_t i0 = threadIdx.x; i0 < P / 2; i0 += 4u * blockDim.x) {
-          uint32_t lo[4], hi[4];
-          unsigned long long a[4], b[4];
-          bool ok[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const uint32_t i = i0 + (uint32_t)u * blockDim.x;
-            ok[u] = false;
-            if (i < P / 2) {
-              bitonicPair(i, k, jj, lo[u], hi[u]);
-              ok[u] = hi[u] < L;
-            }
-            if (ok[u]) {
-              a[u] = V[lo[u]];
-              b[u] = V[hi[u]];
+        if (inShared) {
+          for (uint32_t i = threadIdx.x; i < P / 2; i += blockDim.x) {
+            uint32_t lo, hi;
+            bitonicPair(i, k, jj, lo, hi);
+            if (hi < L) {
+              const unsigned long long a = V[lo], b = V[hi];
+              if (b < a) {
+                V[lo] = b;
+                V[hi] = a;
+                const uint32_t t = I[lo];
+                I[lo] = I[hi];
+                I[hi] = t;
+              }
             }
           }
+        } else {
+          // in global memory (beyond kLargeRow objects: a breakup's fragment
+          // cloud): the comparators of a stage touch disjoint pairs, so each
+          // thread loads four pairs before it compares any (four loads in flight)
+          for (uint32_t i0 = threadIdx.x; i0 < P / 2; i0 += 4u * blockDim.x) {
+            uint32_t lo[4], hi[4];
+            unsigned long long a[4], b[4];
+            bool ok[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (ok[u] && b[u] < a[u]) {
-              V[lo[u]] = b[u];
-              V[hi[u]] = a[u];
-              const uint32_t t = I[lo[u]];
-              I[lo[u]] = I[hi[u]];
-              I[hi[u]] = t;
+            for (int u = 0; u < 4; ++u) {
+              const uint32_t i = i0 + (uint32_t)u * blockDim.x;
+              ok[u] = false;
+              if (i < P / 2) {
+                bitonicPair(i, k, jj, lo[u], hi[u]);
+                ok[u] = hi[u] < L;
+              }
+              if (ok[u]) {
+                a[u] = V[lo[u]];
+                b[u] = V[hi[u]];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              if (ok[u] && b[u] < a[u]) {
+                V[lo[u]] = b[u];
+                V[hi[u]] = a[u];
+                const uint32_t t = I[lo[u]];
+                I[lo[u]] = I[hi[u]];
+                I[hi[u]] = t;
+              }
             }
           }
         }

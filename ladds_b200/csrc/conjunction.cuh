@@ -291,6 +291,23 @@ __global__ void k_burnup_flags(const double *__restrict__ x, const double *__res
   if (below && (threadIdx.x & 31) == 0) atomicAdd(burnt, (unsigned)__popc(below));
 }
 
+// (slot, id) of every object with keep[j] == 0, appended in any order to
+// outSlot / outIdLo / outIdHi (count[0] = their number): the ids of a removal
+// go to the host without copying population-sized arrays.
+__global__ void k_removed_ids(const uint32_t *__restrict__ keep, const uint32_t *__restrict__ tag,
+                              const uint64_t *__restrict__ idBySlot, int n, uint32_t *__restrict__ outSlot,
+                              uint32_t *__restrict__ outIdLo, uint32_t *__restrict__ outIdHi,
+                              unsigned *__restrict__ count) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || keep[j]) return;
+  const uint32_t slot = tagSlot(tag[j]);
+  const uint32_t q = atomicAdd(count, 1u);
+  const uint64_t id = slot < (uint32_t)n ? idBySlot[slot] : 0ull;
+  outSlot[q] = slot;
+  outIdLo[q] = (uint32_t)id;
+  outIdHi[q] = (uint32_t)(id >> 32);
+}
+
 // keep[j] = 0 for the objects that leave the container: a position or
 // velocity that is not finite, or a position outside [boxMin, boxMax]
 // (AutoPas::updateContainer's leaving particles, Simulation.cpp:314; a NaN

@@ -569,7 +569,7 @@ void enqueueSort(ladds_gpu_ctx *c) {
     k_bucket_sort_small<<<smallBlocks, kBucketThreads, 0, c->st>>>(
         c->rowStart, nRows, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff);
   }
-  k_bucket_sort_large<<<c->evalBlocks / 2, kLargeRowThreads, kLargeRow * 12, c->st>>>(
+  k_bucket_sort_large<<<c->evalBlocks / 2, kBucketThreads, kLargeRow * 12, c->st>>>(
       c->rowStart, nx, c->sortRec, c->vals0, c->keys1, c->vals1, c->longRows, c->longCount, c->cellOff, dense);
   c->sortedKeys = c->keys1;
   c->perm = c->vals1;
@@ -607,17 +607,27 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
     // the largest separation a record or a near-band flag can have, with room for rounding
     const double reach = std::sqrt(sc.cutoffSq) * (1.0 + sc.nearRel) * (1.0 + 1e-6);
-    HalfShellRows rows;
-    buildHalfShellRows(rows, c->grid.reach, c->grid.cellSize, reach * reach);
-    const bool r1 = c->grid.reach == 1 && rows.n == 5;  // the five reach-1 rows, all of half-width 1
-    auto walk = buffer ? (r1 ? k_pair_candidates<LADDS_SCREEN_BUFFER, true>
-                             : k_pair_candidates<LADDS_SCREEN_BUFFER, false>)
-                       : (r1 ? k_pair_candidates<LADDS_SCREEN_LISTS, true>
-                             : k_pair_candidates<LADDS_SCREEN_LISTS, false>);
-    walk<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart,
-                                                        c->cellOff, c->grid, cutF, reach * reach,
-                                                        dense.cells ? dense.minCount : 0xffffffffu, c->denseCount,
-                                                        rows, out);
+    const uint32_t denseMin = dense.cells ? dense.minCount : 0xffffffffu;
+    const int form = c->cfg.walkForm != LADDS_WALK_AUTO
+                         ? c->cfg.walkForm
+                         : (!buffer && c->grid.reach == 1 ? LADDS_WALK_GROUPED : LADDS_WALK_ROWS);
+    if (form == LADDS_WALK_ROWS) {
+      (buffer ? k_pair_rows<LADDS_SCREEN_BUFFER> : k_pair_rows<LADDS_SCREEN_LISTS>)<<<blocksFor(c->n, kScanCta),
+                                                                                       kScanCta, 0, s>>>(
+          c->cur.tag, c->posf, (int)c->n, c->sortedKeys, c->rowStart, c->cellOff, c->grid, cutF, reach * reach,
+          denseMin, c->denseCount, out);
+    } else {
+      HalfShellRows rows;
+      buildHalfShellRows(rows, c->grid.reach, c->grid.cellSize, reach * reach);
+      const bool r1 = c->grid.reach == 1 && rows.n == 5;  // the five reach-1 rows, all of half-width 1
+      auto walk = buffer ? (r1 ? k_pair_candidates<LADDS_SCREEN_BUFFER, true>
+                               : k_pair_candidates<LADDS_SCREEN_BUFFER, false>)
+                         : (r1 ? k_pair_candidates<LADDS_SCREEN_LISTS, true>
+                               : k_pair_candidates<LADDS_SCREEN_LISTS, false>);
+      walk<<<blocksFor(c->n, kScanCta), kScanCta, 0, s>>>(c->cur.tag, c->posf, (int)c->n, c->sortedKeys,
+                                                          c->rowStart, c->cellOff, c->grid, cutF, reach * reach,
+                                                          denseMin, c->denseCount, rows, out);
+    }
     if (dense.cells)  // the dense bin: grid-stride over the listed cells (count read on the device)
       (buffer ? k_pair_tiles<LADDS_SCREEN_BUFFER>
               : k_pair_tiles<LADDS_SCREEN_LISTS>)<<<4 * c->evalBlocks, kScanCta, 0, s>>>(
@@ -862,6 +872,7 @@ void ladds_gpu_config_default(ladds_gpu_config *f) {
   f->useGraphs = 1;
   f->pairCapacity = 0;
   f->scanScreen = LADDS_SCREEN_LISTS;
+  f->walkForm = LADDS_WALK_AUTO;
 }
 
 const char *ladds_gpu_last_error(const ladds_gpu_ctx *c) { return c ? c->err.c_str() : "null context"; }
@@ -875,7 +886,8 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
     return LADDS_ERR_INVALID_ARG;
   if (f->propagateBlock < 0 || f->propagateBlock > 256 || (f->propagateBlock % 32) || f->scanBlock < 0 ||
       f->scanBlock > 256 || (f->scanBlock % 32) ||
-      (f->scanScreen != LADDS_SCREEN_LISTS && f->scanScreen != LADDS_SCREEN_BUFFER))
+      (f->scanScreen != LADDS_SCREEN_LISTS && f->scanScreen != LADDS_SCREEN_BUFFER) ||
+      (f->walkForm != LADDS_WALK_AUTO && f->walkForm != LADDS_WALK_GROUPED && f->walkForm != LADDS_WALK_ROWS))
     return LADDS_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -1834,6 +1846,40 @@ int ladds_gpu_mark_deleted(ladds_gpu_ctx *c, const uint32_t *slots, size_t m) {
   return LADDS_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// ids of the objects flagged keep[j] == 0 in scratchA, in slot order (at most
+// cap of them), gathered on the device: only the removed ones cross to the host
+int removedIdsInSlotOrder(ladds_gpu_ctx *c, uint64_t *removedIds, size_t cap) {
+  const int n = (int)c->n;
+  unsigned *dCnt = reinterpret_cast<unsigned *>(c->dCandNeed) + 1;  // word 0 holds the removal count
+  CK(cudaMemsetAsync(dCnt, 0, sizeof(unsigned), c->st));
+  // keys0 / vals0 / scratchB are free between calls (scratchB is compactKept's output, written later)
+  k_removed_ids<<<blocksFor(n, 256), 256, 0, c->st>>>(c->scratchA, c->cur.tag, c->cur.id, n, c->keys0, c->vals0,
+                                                       c->scratchB, dCnt);
+  CK(cudaGetLastError());
+  unsigned m = 0;
+  CK(cudaMemcpyAsync(&m, dCnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  std::vector<uint32_t> sl(m), lo(m), hi(m);
+  if (m) {
+    CK(cudaMemcpyAsync(sl.data(), c->keys0, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(lo.data(), c->vals0, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(hi.data(), c->scratchB, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  std::vector<uint32_t> order(m);
+  for (uint32_t i = 0; i < m; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sl[a] < sl[b]; });
+  for (size_t w = 0; w < m && w < cap; ++w) removedIds[w] = ((uint64_t)hi[order[w]] << 32) | lo[order[w]];
+  return LADDS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemoved, uint64_t *removedIds,
                            size_t cap) {
   if (!c || !std::isfinite(minAltitude)) return LADDS_ERR_INVALID_ARG;
@@ -1854,13 +1900,8 @@ int ladds_gpu_remove_below(ladds_gpu_ctx *c, double minAltitude, size_t *nRemove
   CK(cudaGetLastError());
   if (!burnt) return LADDS_OK;  // nothing burns up: the state, its order and the captured graphs stay
   if (removedIds) {  // ids of the removed objects, in slot order, before the compaction renumbers them
-    std::vector<uint32_t> alive(n);
-    std::vector<uint64_t> ids(n);
-    CK(cudaMemcpy(alive.data(), c->scratchC, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ids.data(), c->cur.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    size_t w = 0;
-    for (int i = 0; i < n && w < cap; ++i)
-      if (!alive[i]) removedIds[w++] = ids[i];
+    const int rid = removedIdsInSlotOrder(c, removedIds, cap);
+    if (rid) return rid;
   }
   int rc = compactKept(c);
   if (rc) return rc;
@@ -1886,13 +1927,8 @@ int ladds_gpu_remove_escaping(ladds_gpu_ctx *c, size_t *nRemoved, uint64_t *remo
   CK(cudaGetLastError());
   if (!escaped) return LADDS_OK;  // nobody leaves: the state, its order and the captured graphs stay
   if (removedIds) {  // ids of the removed objects, in slot order, before the compaction renumbers them
-    std::vector<uint32_t> alive(n);
-    std::vector<uint64_t> ids(n);
-    CK(cudaMemcpy(alive.data(), c->scratchC, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ids.data(), c->cur.id, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    size_t w = 0;
-    for (int i = 0; i < n && w < cap; ++i)
-      if (!alive[i]) removedIds[w++] = ids[i];
+    const int rid = removedIdsInSlotOrder(c, removedIds, cap);
+    if (rid) return rid;
   }
   int rc = compactKept(c);
   if (rc) return rc;
@@ -2147,6 +2183,7 @@ int tuneTrial(ladds_gpu_ctx *c, const ladds_gpu_config &cfg, int chunk, int step
     t.scanBlock = cfg.scanBlock;
     t.chunkSteps = chunk;
     t.scanScreen = cfg.scanScreen;
+    t.walkForm = cfg.walkForm;
     t.msPerStep = st.deviceMs / std::max(steps, 1);
   }
   ladds_gpu_destroy(tc);
@@ -2183,12 +2220,14 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
   //    decides), at the current cell edge
   {
     const ladds_gpu_config base = cfg;
-    for (int screen : {LADDS_SCREEN_LISTS, LADDS_SCREEN_BUFFER}) {
-      ladds_gpu_config k = base;
-      k.scanScreen = screen;
-      const int rc = run(k, bestChunk);
-      if (rc) return rc;
-    }
+    for (int screen : {LADDS_SCREEN_LISTS, LADDS_SCREEN_BUFFER})
+      for (int walk : {LADDS_WALK_GROUPED, LADDS_WALK_ROWS}) {
+        ladds_gpu_config k = base;
+        k.scanScreen = screen;
+        k.walkForm = walk;
+        const int rc = run(k, bestChunk);
+        if (rc) return rc;
+      }
   }
   // 1. cell edge in [20, 160] km: cutoff / R (neighbour reach R = 1..4) and
   //    coarser cells 1.5 and 2 cutoffs wide (reach 1); the current edge is
@@ -2243,6 +2282,7 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
   c->cfg.propagateBlock = cfg.propagateBlock;
   c->cfg.scanBlock = cfg.scanBlock;
   c->cfg.scanScreen = cfg.scanScreen;
+  c->cfg.walkForm = cfg.walkForm;
   c->chunkSteps = bestChunk;
   dropGraphs(c);
   if (regrid) {

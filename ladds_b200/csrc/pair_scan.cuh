@@ -234,9 +234,106 @@ __device__ __forceinline__ void warpWindowPairs(uint32_t lo, uint32_t hi, int la
     const int owner = windowOwner(excl, item);
     const uint32_t oLo = __shfl_sync(0xffffffffu, lo, owner), oEx = __shfl_sync(0xffffffffu, excl, owner);
     const uint32_t jj = (uint32_t)(warpBase + owner), k = oLo + (item - oEx);
-    const bool pass = item < total && prefilterPass(__ldg(&posf[jj]), __ldg(&posf[k]), cutF);
+    bool pass = item < total && prefilterPass(__ldg(&posf[jj]), __ldg(&posf[k]), cutF);
+    if (pass && out.grp) {  // fragments of one breakup never yield a record
+      const uint32_t g = __ldg(&out.grp[jj]);
+      pass = g == kNoGroup || g != __ldg(&out.grp[k]);
+    }
     warpAppend<SCREEN>(pass, jj, k, lane, sCandW, nBuf, out);
   }
+}
+
+// Per-row walk (LADDS_WALK_ROWS): the form for dense populations.  The warp
+// takes the half-shell rows one at a time: every lane locates its window in
+// the row, the windows are concatenated and dealt out 32 items per round with
+// the owner of an item found by a search over the lanes' prefix (few rounds
+// per row: many items per window).  Same pre-filter, screen, group skip and
+// output as the grouped walk below; cutF as there.  The loops over the
+// neighbour rows are warp-uniform; inactive lanes contribute empty windows.
+template <int SCREEN>
+__global__ void __launch_bounds__(kScanCta) k_pair_rows(const uint32_t *__restrict__ tags,
+                                                              const float4 *__restrict__ posf, int n,
+                                                              const uint32_t *__restrict__ skeys,
+                                                              const uint32_t *__restrict__ rowStart,
+                                                              const uint16_t *__restrict__ cellOff, GridDesc g,
+                                                              float cutF, double reachR2, uint32_t denseMin,
+                                                              const uint32_t *__restrict__ denseCount,
+                                                              const CandSink out) {
+  __shared__ uint2 sCand[kScanCta / 32][kWarpCand];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
+  const int warpBase = blockIdx.x * kScanCta + warp * 32;
+  const int j = warpBase + lane;
+  const bool inRange = j < n;
+  const uint32_t myTag = inRange ? tags[j] : kTagDummy;
+  bool active = inRange && !tagDummy(myTag) && tagSlot(myTag) < out.haloStart;
+  const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
+  int32_t ix = 0, iy = 0, iz = 0;
+  if (active) {
+    const uint32_t key = skeys[j];
+    ix = (int32_t)(key % (uint32_t)nx);
+    const uint32_t row = key / (uint32_t)nx;
+    iy = (int32_t)(row % (uint32_t)ny);
+    iz = (int32_t)(row / (uint32_t)ny);
+    // objects of the dense bin (own cell >= denseMin objects) are scanned by k_pair_tiles
+    if (cellOff && denseMin != 0xffffffffu && __ldg(denseCount) != 0u) {
+      uint32_t a, b;  // the own cell's objects (rows beyond 16-bit offsets: searched)
+      rowWindow(row, (uint32_t)ix, (uint32_t)ix, (uint32_t)nx, rowStart, cellOff, skeys, a, b);
+      if (b - a >= denseMin) active = false;
+    }
+  }
+  const double c2 = g.cellSize * g.cellSize;
+  // Dense populations (the buffer form) with cells below the cutoff (reach >=
+  // 2): the object's own x-window in
+  // each neighbour row: partners lie within reachF of it, and a row whose
+  // (y, z) cell box is dyMin, dzMin away can hold them only within
+  // hw = sqrt(reachF^2 - dyMin^2 - dzMin^2) of its x.  Binary32 geometry with a
+  // 50 m margin over the pre-filter radius (which dwarfs the rounding of
+  // positions and cell edges); offsets inside the own cell are clamped to the
+  // cell, which only widens the windows of objects clamped into boundary
+  // cells.  With reach 1, or sparse populations (the list form), the cell
+  // windows are kept: trimming them does not pay for its arithmetic.
+  const bool perObject = SCREEN == LADDS_SCREEN_BUFFER && R >= 2;  // warp-uniform
+  const float4 me = active && perObject ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float cf = (float)g.cellSize, invCf = (float)g.invCell;
+  const float fy = fminf(fmaxf(me.y - ((float)g.boxMin[1] + (float)iy * cf), 0.f), cf);
+  const float fz = fminf(fmaxf(me.z - ((float)g.boxMin[2] + (float)iz * cf), 0.f), cf);
+  const float xRel = me.x - (float)g.boxMin[0];
+  const float reachF = cutF + 0.05f, reachF2 = reachF * reachF;
+  for (int dz = 0; dz <= R; ++dz) {
+    const float dzMin = dz == 0 ? 0.f : (float)(dz - 1) * cf + (cf - fz);
+    for (int dy = (dz == 0 ? 0 : -R); dy <= R; ++dy) {
+      const int w = rowHalfWidth(dy, dz, R, c2, reachR2);  // warp-uniform
+      if (w < 0) continue;
+      const int32_t jz = iz + dz, jy = iy + dy;
+      int32_t lo32 = dz == 0 && dy == 0 ? ix : max(ix - w, 0), hi32 = min(ix + w, nx - 1);
+      bool inReach = true;
+      if (perObject) {
+        const float dyMin =
+            dy == 0 ? 0.f : dy > 0 ? (float)(dy - 1) * cf + (cf - fy) : (float)(-dy - 1) * cf + fy;
+        const float h2 = reachF2 - dyMin * dyMin - dzMin * dzMin;
+        const float hw = h2 > 0.f ? h2 * rsqrtf(h2) : 0.f;
+        if (!(dz == 0 && dy == 0)) lo32 = max(lo32, (int32_t)floorf((xRel - hw) * invCf));
+        hi32 = min(hi32, (int32_t)floorf((xRel + hw) * invCf));
+        inReach = h2 >= 0.f && hi32 >= lo32;
+      }
+      const bool ok = active && jz < nz && jy >= 0 && jy < ny && inReach;
+      const uint32_t r2 = ok ? (uint32_t)jz * (uint32_t)ny + (uint32_t)jy : 0u;
+      const uint32_t xlo = ok ? (uint32_t)lo32 : 0u;
+      const uint32_t xhi = ok ? (uint32_t)hi32 : 0u;
+      const RowLookup L = rowLoads(r2, xlo, xhi, (uint32_t)nx, rowStart, cellOff);  // four reads in flight
+      uint32_t lo = 0, hi = 0;
+      if (ok) {
+        rowFinish(L, r2, xlo, xhi, (uint32_t)nx, cellOff, skeys, lo, hi);
+        if (dz == 0 && dy == 0) {  // own cell: later objects only
+          lo = (uint32_t)j + 1u;
+          if (hi < lo) hi = lo;
+        }
+      }
+      warpWindowPairs<SCREEN>(lo, hi, lane, warpBase, posf, cutF, sCand[warp], nBuf, out);
+    }
+  }
+  warpFlush<SCREEN>(lane, sCand[warp], nBuf, out);
 }
 
 // Half-shell rows of a scan: (dz, dy, x half-width w) of every neighbour row

@@ -117,12 +117,13 @@ DENSE_KW = dict(cutoff=20.0, collisionDistanceFactor=2000.0, minDetectionRadius=
                 conjunctionThreshold=2.0, boxMin=DENSE_BOX[0], boxMax=DENSE_BOX[1])
 
 
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("screen", [0, 1])
 @pytest.mark.parametrize("cell", [0.0, 7.0, 10.0, 33.0, 60.0])
-def test_scan_bitexact_vs_oracle(capi, oracle, cell, screen):
+def test_scan_bitexact_vs_oracle(capi, oracle, cell, screen, walk):
     pop = dense_population(11)
     dt = 10.0
-    with ctx_for(capi, cellSize=cell, scanScreen=screen, **DENSE_KW) as ctx:
+    with ctx_for(capi, cellSize=cell, scanScreen=screen, walkForm=walk, **DENSE_KW) as ctx:
         ctx.upload(pop)
         recs = ctx.conjunctions(dt)
         keys, slots = ctx.cell_order()
@@ -395,9 +396,10 @@ def fragment_clouds(seed):
     return pop
 
 
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("screen", [0, 1])
 @pytest.mark.parametrize("cell", [0.0, 7.0])
-def test_breakup_clouds_bitexact_vs_oracle(capi, oracle, cell, screen):
+def test_breakup_clouds_bitexact_vs_oracle(capi, oracle, cell, screen, walk):
     """Fragments of one breakup start at one point: their pairs are skipped
     before they become candidates (whole blocks of one group in the dense-bin
     tiles, single pairs in the walk), the crowded cell is shared out in
@@ -405,7 +407,7 @@ def test_breakup_clouds_bitexact_vs_oracle(capi, oracle, cell, screen):
     functor (CollisionFunctor.cpp:64-67)."""
     pop = fragment_clouds(31)
     dt = 10.0
-    with ctx_for(capi, cellSize=cell, scanScreen=screen, **DENSE_KW) as ctx:
+    with ctx_for(capi, cellSize=cell, scanScreen=screen, walkForm=walk, **DENSE_KW) as ctx:
         ctx.upload(pop)
         recs = ctx.conjunctions(dt)
     p = oracle.scan_params(cutoff=20.0, dt=dt, factor=2000.0, min_detection_radius=0.05, evasion_cutoff=3.0,
