@@ -475,7 +475,8 @@ int ladds_records_write_csv(const char *path, int append, const ladds_pair *recs
  *   0. screening form of full candidate buffers (LADDS_SCREEN_*) x walk form
  *      (LADDS_WALK_GROUPED / _ROWS) at the current cell edge;
  *   1. cell edge: the current one, cutoff / R for reach R = 1..4 and 1.5 and 2
- *      cutoffs, those within [20, 160] km;
+ *      cutoffs, those within [20, 160] km; then the other walk form at the
+ *      chosen edge;
  *   2. propagateBlock x scanBlock in {128, 256}^2;
  *   3. iterations per captured chunk (graph) in {32, 64, 128}.
  * Results never depend on these (the scan is exact for any cell edge, records

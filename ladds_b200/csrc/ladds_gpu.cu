@@ -2249,6 +2249,15 @@ int ladds_gpu_autotune(ladds_gpu_ctx *c, int stepsPerTrial, ladds_tune_trial *tr
       if (rc) return rc;
     }
   }
+  // 1b. the other walk form at the chosen cell edge (the form that suits a
+  //     cell edge depends on the items per window, which the edge sets)
+  {
+    const ladds_gpu_config base = cfg;
+    ladds_gpu_config k = base;
+    k.walkForm = base.walkForm == LADDS_WALK_ROWS ? LADDS_WALK_GROUPED : LADDS_WALK_ROWS;
+    const int rc = run(k, bestChunk);
+    if (rc) return rc;
+  }
   // 2. block shapes of the propagation and of the pair evaluation
   {
     const ladds_gpu_config base = cfg;
