@@ -549,10 +549,14 @@ void enqueueSort(ladds_gpu_ctx *c) {
   const int n = (int)c->n;
   const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
   {
-    PhaseScope ps(c, kPhBucket, c->st, 1 + exclusiveScanKernels((size_t)nRows + 1));
+    const bool single = (size_t)nRows + 1 <= (size_t)kScanSingleMax;  // the row starts in one launch
+    PhaseScope ps(c, kPhBucket, c->st, 1 + (single ? 1 : exclusiveScanKernels((size_t)nRows + 1)));
     cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
     cudaMemsetAsync(c->denseCount, 0, sizeof(uint32_t), c->st);
-    enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
+    if (single)
+      k_scan_single<<<1, kScanBlock, kScanSingleSmem, c->st>>>(c->rowCounts, (int)nRows + 1, c->rowStart);
+    else
+      enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
     k_bucket_place<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
         c->keys0, c->scratchC, c->cur.tag, n, nx, c->rowStart, c->sortRec, c->vals0, c->dStatus);
   }
@@ -933,6 +937,13 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
     cudaGetLastError();
     ladds_gpu_destroy(c);
     return LADDS_ERR_ALLOC;
+  }
+  // the single-CTA row-start scan stages 128 KB of counts in shared memory
+  if (cudaFuncSetAttribute(k_scan_single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSingleSmem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    ladds_gpu_destroy(c);
+    return LADDS_ERR_CUDA;
   }
   c->dIterBase = c->dIter + 1;
   // record count, largest candidate count and status words side by side: one read after a step

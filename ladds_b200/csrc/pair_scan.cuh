@@ -418,26 +418,29 @@ __global__ void __launch_bounds__(kScanCta) k_pair_candidates(const uint32_t *__
   const int warpBase = blockIdx.x * kScanCta + warp * 32;
   const int j = warpBase + lane;
   const bool inRange = j < n;
+  // the object's own reads, all issued before any of them is used
   const uint32_t myTag = inRange ? tags[j] : kTagDummy;
+  const uint32_t key = inRange ? skeys[j] : 0u;
+  const float4 me = inRange ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t myGrp = out.grp && inRange ? __ldg(&out.grp[j]) : kNoGroup;
+  const bool denseOn = cellOff && denseMin != 0xffffffffu && __ldg(denseCount) != 0u;
   bool active = inRange && !tagDummy(myTag) && tagSlot(myTag) < out.haloStart;
   const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
   int32_t ix = 0, iy = 0, iz = 0;
   if (active) {
-    const uint32_t key = skeys[j];
     ix = (int32_t)(key % (uint32_t)nx);
     const uint32_t row = key / (uint32_t)nx;
     iy = (int32_t)(row % (uint32_t)ny);
     iz = (int32_t)(row / (uint32_t)ny);
     // objects of the dense bin (own cell >= denseMin objects) are scanned by k_pair_tiles
-    if (cellOff && denseMin != 0xffffffffu && __ldg(denseCount) != 0u) {
+    if (denseOn) {
       uint32_t a, b;  // the own cell's objects (rows beyond 16-bit offsets: searched)
       rowWindow(row, (uint32_t)ix, (uint32_t)ix, (uint32_t)nx, rowStart, cellOff, skeys, a, b);
       if (b - a >= denseMin) active = false;
     }
   }
-  const float4 me = inRange ? __ldg(&posf[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
   sOwn[warp][lane] = me;
-  if (out.grp) sGrp[warp][lane] = inRange ? __ldg(&out.grp[j]) : kNoGroup;
+  if (out.grp) sGrp[warp][lane] = myGrp;
   const double c2 = g.cellSize * g.cellSize;
   // Dense populations (the buffer form) with cells below the cutoff (reach >=
   // 2): the object's own x-window in each neighbour row: partners lie within
