@@ -9,8 +9,12 @@ the 80 km cell-list cutoff and the 0.1 km conjunction threshold.
 One step = one iteration of the reference loop (Simulation.cpp:287-415):
 Yoshida-4 step of every object, then the conjunction scan.  ``value`` is the
 split-precision object-steps/s with the population resident in HBM; the FP64
-figure, their ratio and the one-day RMS drift of split vs FP64 are reported
-beside it.  ``e2e`` runs the same steps through the C ABI in the host-owned
+figure and their ratio are reported beside it, and further legs measure:
+split vs FP64 per population (position drift and the conjunction sets compared
+pair by pair), the constellation and 8e6 scale populations (autotuned), the
+adjoint of 4096 conjunction pairs with its finite-difference check, and the 8e6
+population's breakups over one day.  The line ends with ``north_star``, a
+summary of those figures.  ``e2e`` runs the same steps through the C ABI in the host-owned
 mode of the drop-in (ladds_gpu_step_host): per step the positions/velocities
 go host->device from pinned memory, the step runs, positions/velocities and
 the conjunction records come back; ``e2e.device_resident`` is the drop-in's own data flow, the

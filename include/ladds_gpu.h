@@ -107,7 +107,9 @@ typedef struct {
   double cellSize;                /* cell edge [km]; <= 0 means = cutoff               */
   double boxMin[3], boxMax[3];    /* cell-grid box [km]; objects outside are clamped   */
   int32_t device;                 /* CUDA device ordinal                               */
-  int32_t propagateBlock;         /* threads per block of the propagation kernel (0: 256) */
+  int32_t propagateBlock;         /* threads per block of the multi-step propagation kernel
+                                     (0: 256); the propagation before a scan runs a
+                                     persistent kernel of 256-object tiles */
   int32_t scanBlock;              /* threads per block of the candidate evaluation (0: 256) */
   int32_t useGraphs;              /* capture multi-iteration calls in CUDA graphs      */
   uint64_t pairCapacity;          /* initial device pair-buffer capacity (0: auto)     */

@@ -397,59 +397,6 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const uint32_t *__re
   if (i < n) out[i] = off + incl - v;
   if (threadIdx.x == kScanBlock - 1) blockSums[blockIdx.x] = off + incl;
 }
-// Exclusive scan of at most kScanSingleMax entries by one CTA (the row-start
-// table of grids up to 2^16 rows): passes of kScanTile entries staged in
-// shared memory (coalesced reads, 32 entries per thread with one pad word per
-// 32 so that the threads' runs start in different banks), one block scan per
-// pass, a running carry between passes.  One launch instead of three.
-constexpr int kScanTile = 32 * kScanBlock;
-constexpr int kScanSingleMax = 2 * kScanTile;
-constexpr size_t kScanSingleSmem = (size_t)(kScanTile + kScanTile / 32 + 32) * sizeof(uint32_t);
-__global__ void __launch_bounds__(kScanBlock) k_scan_single(const uint32_t *__restrict__ in, int n,
-                                                            uint32_t *__restrict__ out) {
-  extern __shared__ uint32_t sm[];
-  uint32_t *ws = sm + kScanTile + kScanTile / 32;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  auto at = [](int i) { return i + (i >> 5); };
-  uint32_t carry = 0;
-  for (int base = 0; base < n; base += kScanTile) {
-    const int m = min(kScanTile, n - base);
-    for (int i = t; i < kScanTile; i += kScanBlock) sm[at(i)] = i < m ? in[base + i] : 0u;
-    __syncthreads();
-    uint32_t sum = 0;
-#pragma unroll 8
-    for (int k = 0; k < 32; ++k) sum += sm[at(t * 32 + k)];
-    uint32_t incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    if (lane == 31) ws[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t w = ws[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += v;
-      }
-      ws[lane] = w;
-    }
-    __syncthreads();
-    uint32_t run = carry + (warp ? ws[warp - 1] : 0u) + incl - sum;
-#pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
-      const uint32_t v = sm[at(t * 32 + k)];
-      sm[at(t * 32 + k)] = run;
-      run += v;
-    }
-    carry += ws[31];
-    __syncthreads();
-    for (int i = t; i < m; i += kScanBlock) out[base + i] = sm[at(i)];
-    __syncthreads();
-  }
-}
 
 __global__ void k_scan_add(uint32_t *__restrict__ out, int n, const uint32_t *__restrict__ blockOffsets) {
   const int i = blockIdx.x * kScanBlock + threadIdx.x;

@@ -459,6 +459,14 @@ cudaError_t enqueueEphemeris(ladds_gpu_ctx *c, int nSteps) {
                                  c->st);
 }
 
+// the bulk copies of k_propagate_staged need 16-byte aligned arrays
+bool stageable(const DevState &s) {
+  const void *p[] = {s.x, s.y, s.z, s.vx, s.vy, s.vz, s.aom, s.bc, s.tag};
+  for (const void *q : p)
+    if (reinterpret_cast<uintptr_t>(q) & 15u) return false;
+  return true;
+}
+
 // the propagation kernel over objects [0, n) of s on the main stream; with
 // keys, their cell keys and row arrivals go to keyOut / arrOut (indexed as s)
 void launchPropagate(ladds_gpu_ctx *c, const DevState &s, int n, int nSteps, int ephBase, bool keys,
@@ -466,6 +474,16 @@ void launchPropagate(ladds_gpu_ctx *c, const DevState &s, int n, int nSteps, int
   const int b = c->cfg.propagateBlock > 0 ? c->cfg.propagateBlock : 256;
   const int g = blocksFor((size_t)n, b);
   uint32_t *rc = c->rowCounts;
+  if (keys && stageable(s)) {  // the per-scan propagation: persistent grid, state staged by bulk copies
+    const int sg = std::max(1, std::min(blocksFor((size_t)n, kStageObjects), c->evalBlocks));
+    if (c->cfg.precision == LADDS_PRECISION_SPLIT)
+      k_propagate_staged<true><<<sg, kStageObjects, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc,
+                                                                arrOut, c->dStatus);
+    else
+      k_propagate_staged<false><<<sg, kStageObjects, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc,
+                                                                 arrOut, c->dStatus);
+    return;
+  }
   if (c->cfg.precision == LADDS_PRECISION_SPLIT) {
     if (keys)
       k_propagate<true, true><<<g, b, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc, arrOut,
@@ -549,14 +567,10 @@ void enqueueSort(ladds_gpu_ctx *c) {
   const int n = (int)c->n;
   const uint32_t nx = (uint32_t)c->grid.n[0], nRows = c->nRows;
   {
-    const bool single = (size_t)nRows + 1 <= (size_t)kScanSingleMax;  // the row starts in one launch
-    PhaseScope ps(c, kPhBucket, c->st, 1 + (single ? 1 : exclusiveScanKernels((size_t)nRows + 1)));
+    PhaseScope ps(c, kPhBucket, c->st, 1 + exclusiveScanKernels((size_t)nRows + 1));
     cudaMemsetAsync(c->longCount, 0, sizeof(uint32_t), c->st);
     cudaMemsetAsync(c->denseCount, 0, sizeof(uint32_t), c->st);
-    if (single)
-      k_scan_single<<<1, kScanBlock, kScanSingleSmem, c->st>>>(c->rowCounts, (int)nRows + 1, c->rowStart);
-    else
-      enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
+    enqueueExclusiveScan(c, c->rowCounts, (size_t)nRows + 1, c->rowStart);
     k_bucket_place<<<blocksFor(c->n, kBucketThreads), kBucketThreads, 0, c->st>>>(
         c->keys0, c->scratchC, c->cur.tag, n, nx, c->rowStart, c->sortRec, c->vals0, c->dStatus);
   }
@@ -706,6 +720,7 @@ int syncAndStatus(ladds_gpu_ctx *c) {
   CK(cudaMemcpy(&status, c->dStatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
   if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
+  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait ran out (staged propagation)");
   if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
   return LADDS_OK;
 }
@@ -719,6 +734,7 @@ int syncStatusAndGrow(ladds_gpu_ctx *c, unsigned long long *records, bool *overf
   const unsigned status = (unsigned)(w[2] & 0xffffffffull);
   if (status) CK(cudaMemset(c->dStatus, 0, sizeof(unsigned)));
   if (status & 4u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a device-side index check failed (sort / gather)");
+  if (status & 8u) return fail(c, LADDS_ERR_DEVICE_CHECK, "a bounded device wait ran out (staged propagation)");
   if (status & 1u) return fail(c, LADDS_ERR_NONFINITE, "a position or velocity became NaN/Inf during propagation");
   *records = w[0];
   *overflow = w[0] > c->pairCap || w[1] > c->candCap;
@@ -937,13 +953,6 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
     cudaGetLastError();
     ladds_gpu_destroy(c);
     return LADDS_ERR_ALLOC;
-  }
-  // the single-CTA row-start scan stages 128 KB of counts in shared memory
-  if (cudaFuncSetAttribute(k_scan_single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSingleSmem) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    ladds_gpu_destroy(c);
-    return LADDS_ERR_CUDA;
   }
   c->dIterBase = c->dIter + 1;
   // record count, largest candidate count and status words side by side: one read after a step
@@ -1684,7 +1693,8 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
   }
   // chunks: host->device on st2, propagation on st, device->host on st3
   const int chunks = (int)std::max<size_t>(1, std::min<size_t>((size_t)kHostChunks, n / kHostChunkMin));
-  const size_t per = (n + (size_t)chunks - 1) / (size_t)chunks;
+  // chunk starts on multiples of 256 objects keep every chunk's arrays 16-byte aligned (staged propagation)
+  const size_t per = ((n + (size_t)chunks - 1) / (size_t)chunks + 255) / 256 * 256;
   double *const sArr[6] = {S.x, S.y, S.z, S.vx, S.vy, S.vz};
   int used = 0;
   for (int ch = 0; ch < chunks && n; ++ch) {
