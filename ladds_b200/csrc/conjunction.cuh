@@ -60,20 +60,22 @@ __global__ void k_permute(DevState src, DevState dst, const uint32_t *__restrict
     atomicOr(status, 4u);
     p = (uint32_t)j;
   }
-  const double x = src.x[p], y = src.y[p], z = src.z[p];
-  const double vx = src.vx[p], vy = src.vy[p], vz = src.vz[p];
-  const uint32_t tag = src.tag[p];
-  const double radius = tagSlot(tag) < (uint32_t)n ? src.radius[tagSlot(tag)] : 0.0;  // slot-indexed
+  // read-only loads; the gathered state is written with streaming stores (it
+  // is read once, by the next propagation), the scan copies with plain ones
+  const double x = __ldg(&src.x[p]), y = __ldg(&src.y[p]), z = __ldg(&src.z[p]);
+  const double vx = __ldg(&src.vx[p]), vy = __ldg(&src.vy[p]), vz = __ldg(&src.vz[p]);
+  const uint32_t tag = __ldg(&src.tag[p]);
+  const double radius = tagSlot(tag) < (uint32_t)n ? __ldg(&src.radius[tagSlot(tag)]) : 0.0;  // slot-indexed
   if (pk.grp) pk.grp[j] = tagSlot(tag) < (uint32_t)n ? groupOf(src.parent[tagSlot(tag)]) : kNoGroup;
-  dst.x[j] = x;
-  dst.y[j] = y;
-  dst.z[j] = z;
-  dst.vx[j] = vx;
-  dst.vy[j] = vy;
-  dst.vz[j] = vz;
-  dst.aom[j] = src.aom[p];
-  dst.bc[j] = src.bc[p];
-  dst.tag[j] = tag;
+  __stcs(&dst.x[j], x);
+  __stcs(&dst.y[j], y);
+  __stcs(&dst.z[j], z);
+  __stcs(&dst.vx[j], vx);
+  __stcs(&dst.vy[j], vy);
+  __stcs(&dst.vz[j], vz);
+  __stcs(&dst.aom[j], __ldg(&src.aom[p]));
+  __stcs(&dst.bc[j], __ldg(&src.bc[p]));
+  __stcs(&dst.tag[j], tag);
   pk.posf[j] = floatPosition(x, y, z);
   pk.velf[j] = make_float4((float)vx, (float)vy, (float)vz, __double2float_ru(radius));
 }
@@ -396,6 +398,21 @@ __global__ void __launch_bounds__(kScanBlock) k_scan_blocks(const uint32_t *__re
   const uint32_t off = warp ? ws[warp - 1] : 0u;
   if (i < n) out[i] = off + incl - v;
   if (threadIdx.x == kScanBlock - 1) blockSums[blockIdx.x] = off + incl;
+}
+
+// second pass of a two-pass exclusive scan (at most kScanBlock blocks): block b
+// adds the sum of blockSums[0, b) -- the scan of the block sums folded into
+// the apply pass
+__global__ void __launch_bounds__(kScanBlock) k_scan_add_prefix(uint32_t *__restrict__ out, int n,
+                                                                const uint32_t *__restrict__ blockSums) {
+  __shared__ uint32_t ws[32];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const uint32_t w = __reduce_add_sync(0xffffffffu, t < b ? blockSums[t] : 0u);
+  if ((t & 31) == 0) ws[t >> 5] = w;
+  __syncthreads();
+  const uint32_t off = __reduce_add_sync(0xffffffffu, ws[t & 31]);  // every warp sums the 32 partials
+  const int i = b * kScanBlock + t;
+  if (i < n && b > 0) out[i] += off;
 }
 
 __global__ void k_scan_add(uint32_t *__restrict__ out, int n, const uint32_t *__restrict__ blockOffsets) {

@@ -515,19 +515,27 @@ void enqueuePropagate(ladds_gpu_ctx *c, int nSteps, bool keys, int ephBase) {
 }
 
 // kernels launched by enqueueExclusiveScan for `count` values
+constexpr bool kScanFoldSums = true;  // two passes up to kScanBlock^2 values (else three)
+
 int exclusiveScanKernels(size_t count) {
   const int nb1 = blocksFor(count, kScanBlock);
   if (nb1 == 1) return 1;
+  if (kScanFoldSums && nb1 <= kScanBlock) return 2;
   return blocksFor((size_t)nb1, kScanBlock) > 1 ? 5 : 3;
 }
 
-// exclusive scan of `count` u32 values (three levels of 1024-wide block scans,
-// count <= 2^30); block sums live in c->scanWs
+// exclusive scan of `count` u32 values (1024-wide block scans; up to 2^20
+// values: block scans, then each block adds the sum of the blocks before it;
+// beyond: three levels, count <= 2^30); block sums live in c->scanWs
 void enqueueExclusiveScan(ladds_gpu_ctx *c, const uint32_t *in, size_t count, uint32_t *out) {
   const int nb1 = blocksFor(count, kScanBlock);
   uint32_t *s1 = c->scanWs, *s1x = s1 + nb1 + 1;
   k_scan_blocks<<<nb1, kScanBlock, 0, c->st>>>(in, (int)count, out, s1);
   if (nb1 == 1) return;
+  if (kScanFoldSums && nb1 <= kScanBlock) {
+    k_scan_add_prefix<<<nb1, kScanBlock, 0, c->st>>>(out, (int)count, s1);
+    return;
+  }
   const int nb2 = blocksFor((size_t)nb1, kScanBlock);
   uint32_t *s2 = s1x + nb1 + 1;
   k_scan_blocks<<<nb2, kScanBlock, 0, c->st>>>(s1, nb1, s1x, s2);
