@@ -314,6 +314,31 @@ def test_propagation_vs_oracle_100_steps(capi, oracle, mask_name, precision):
     assert np.array_equal(got["id"], pop["id"])
 
 
+@pytest.mark.parametrize("k", [1, 3])
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("n", [1, 255, 256, 257, 4096, 70_001])
+def test_staged_propagation_equals_register_kernel(capi, n, precision, k):
+    """The propagation before a scan (persistent grid, 256-object tiles brought
+    into shared memory by bulk copies, the partial last tile read directly)
+    gives the state of the multi-step register kernel bit for bit, with the
+    scan every step and every third step."""
+    pop = capi.generate_population(0, 77, n)
+    pop["activity"][::50] = capi.EVASIVE_PRESERVING
+    states = []
+    for use_step in (False, True):
+        with ctx_for(capi, componentMask=capi.PROP_ALL, precision=precision, useGraphs=0,
+                     timestepsPerCollisionDetection=k) as ctx:
+            ctx.upload(pop)
+            for _ in range(2):
+                if use_step:
+                    ctx.step(k)
+                else:
+                    ctx.integrate(k)
+            states.append(ctx.download())
+    for key in ("x", "y", "z", "vx", "vy", "vz", "id"):
+        assert np.array_equal(states[0][key], states[1][key]), key
+
+
 @pytest.mark.parametrize("screen", [0, 1])
 def test_graph_replay_equals_eager(capi, screen):
     pop = dense_population(14, n=5000)
