@@ -591,7 +591,7 @@ def applied_breakup_run(capi, cfg, bcfg, pop, iterations, min_altitude, wall_bud
 FD_STENCIL = (1.0, -1.0, 0.5, -0.5, 0.25, -0.25)  # multiples of h of the perturbed evaluations
 
 
-def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3):
+def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3, with_classes=False):
     """Finite-difference check of directional derivatives gd (one per pair)
     from the losses f0 at x and fm[k] at x + FD_STENCIL[k] h d, with the argmin
     steps step0 / stepm[k] of each evaluation.
@@ -610,7 +610,8 @@ def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3):
     usable but disagreeing: a kink within h/4 of x, on an unknown side
     ("ambiguous", the closer side's error is reported).  One side usable: that
     side.  Neither: unresolved at this h.  Returns the per-pair relative
-    errors and the counts of each class."""
+    errors and the counts of each class (and, with_classes, the per-pair
+    class masks)."""
     keep = stepm == step0[None, :]
     d = lambda k, t: (fm[k] - f0) / (t * eps)  # one-sided quotient at t h (t may be negative)
     # a side is usable when its three points keep the argmin step and its two
@@ -639,7 +640,35 @@ def fd_classify(gd, f0, fm, step0, stepm, eps, tol=1e-6, consistency=1e-3):
     counts = {"central": int(agree.sum()), "ambiguous": int(kink.sum()), "forward_only": int(only_p.sum()),
               "backward_only": int(only_m.sum()), "unresolved": int(unresolved.sum()),
               "central_meeting_tol": int(np.sum(rel[agree] <= tol))}
+    if with_classes:
+        return rel, counts, {"central": agree, "one_sided": only_p | only_m, "ambiguous": kink}
     return rel, counts
+
+
+FD_LADDER = (1e-6, 1e-7, 1e-8)  # relative step sizes of the finite-difference ladder
+
+
+def fd_ladder(levels, tol=1e-6):
+    """Per pair, the finite-difference value at the largest h of the ladder
+    where it is resolved, in the order central (both sides smooth and
+    agreeing), one-sided, ambiguous (a kink within h/4): a kink of the
+    minimum-over-steps loss that lies inside the stencil at h usually lies
+    outside it at h/10 or h/100, and the binary64 round-off of the quotients
+    stays near 1e-16 |x| / (h |d|) <= 1e-8 of the derivative at h = 1e-8 |x|.
+    levels: [(h_rel, rel, classes)] from fd_classify(..., with_classes=True)."""
+    n = len(levels[0][1])
+    best, level = np.full(n, np.inf), np.full(n, -1)
+    for cls_name in ("central", "one_sided", "ambiguous"):
+        for li, (_, rel, cls) in enumerate(levels):
+            m = (level < 0) & cls[cls_name]
+            best[m], level[m] = rel[m], li
+    fin = best[np.isfinite(best)]
+    return {"h": [h for h, _, _ in levels],
+            "resolved_at": [int(np.sum(level == li)) for li in range(len(levels))],
+            "unresolved": int(np.sum(level < 0)),
+            "meets_1e-6": int(np.sum(best <= tol)), "meets_1e-6_frac": float(np.mean(best <= tol)),
+            "rel_err_median": float(np.median(fin)) if len(fin) else None,
+            "rel_err_p99": float(np.quantile(fin, 0.99)) if len(fin) else None}
 
 
 def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
@@ -647,7 +676,8 @@ def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
     set, checkpoints every 64 steps.  Device times of the forward sweep (loss +
     checkpoints) and of the backward sweep (segment recompute + reverse sweep),
     and a directional finite-difference check of every pair's gradient at
-    h = 1e-6 |x| (and h / 2; fd_classify)."""
+    h = 1e-6 |x| (fd_classify), and per pair at the largest h of 1e-6, 1e-7,
+    1e-8 |x| where it is resolved (fd_ladder)."""
     with capi.Context(capi.default_config(componentMask=capi.PROP_ALL, device=device)) as ctx:
         pairs, _ = ctx.adjoint_make_pairs(77, n_pairs, steps)
         ctx.adjoint_forward(pairs, steps, ck)
@@ -661,30 +691,40 @@ def adjoint_leg(capi, device, n_pairs=4096, steps=1080, ck=64, reps=3):
         rng = np.random.default_rng(3)
         d = rng.normal(size=rows.shape) * np.abs(rows)
         d /= np.linalg.norm(d, axis=1, keepdims=True)
-        eps = 1e-6 * np.linalg.norm(rows, axis=1)
-        batch = []
-        for f in FD_STENCIL:
-            q = pairs.copy()
-            r = rows + f * eps[:, None] * d
-            q["rA"], q["vA"], q["rB"], q["vB"] = r[:, 0:3], r[:, 3:6], r[:, 6:9], r[:, 9:12]
-            batch.append(q)
-        _, miss, stepP, _ = ctx.adjoint_forward(np.concatenate(batch), steps, ck)
         _, miss0, step0, _ = ctx.adjoint_forward(pairs, steps, ck)
-    gd = np.sum(dx * d, axis=1)
-    k = len(FD_STENCIL)
-    rel, counts = fd_classify(gd, miss0, miss.reshape(k, n_pairs), step0, stepP.reshape(k, n_pairs), eps)
+        gd = np.sum(dx * d, axis=1)
+        k = len(FD_STENCIL)
+        levels = []
+        for h_rel in FD_LADDER:
+            eps = h_rel * np.linalg.norm(rows, axis=1)
+            batch = []
+            for f in FD_STENCIL:
+                q = pairs.copy()
+                r = rows + f * eps[:, None] * d
+                q["rA"], q["vA"], q["rB"], q["vB"] = r[:, 0:3], r[:, 3:6], r[:, 6:9], r[:, 9:12]
+                batch.append(q)
+            _, miss, stepP, _ = ctx.adjoint_forward(np.concatenate(batch), steps, ck)
+            lv = fd_classify(gd, miss0, miss.reshape(k, n_pairs), step0, stepP.reshape(k, n_pairs), eps,
+                             with_classes=True)
+            if not levels:
+                rel, counts, _ = lv
+            levels.append((h_rel, lv[0], lv[2]))
+    ladder = fd_ladder(levels)
     fin = rel[np.isfinite(rel)]
     f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
     fd = {"direction": "random per pair, 12 state components, relative scaling", "h": "1e-6 |x|, h/2, h/4",
           "pairs": n_pairs, **counts,
           "meets_1e-6": int(np.sum(rel <= 1e-6)), "meets_1e-6_frac": float(np.mean(rel <= 1e-6)),
           "rel_err_median": float(np.median(fin)) if len(fin) else None,
-          "rel_err_p99": float(np.quantile(fin, 0.99)) if len(fin) else None}
+          "rel_err_p99": float(np.quantile(fin, 0.99)) if len(fin) else None,
+          "ladder": ladder}
     return {"pairs": n_pairs, "steps": steps, "checkpoint_every": ck, "forward_ms": f_ms, "backward_ms": b_ms,
             "backward_over_forward": b_ms / f_ms, "forward_plus_backward_over_forward": (f_ms + b_ms) / f_ms,
             "fd_check": fd,
             "fd_summary": {"meets_1e-6_frac": fd["meets_1e-6_frac"], "unresolved": counts["unresolved"],
-                           "median": fd["rel_err_median"]}}
+                           "median": fd["rel_err_median"],
+                           "ladder_meets_1e-6_frac": ladder["meets_1e-6_frac"],
+                           "ladder_unresolved": ladder["unresolved"]}}
 
 
 # ------------------------------------------------------------------ GPU arm
