@@ -492,6 +492,7 @@ def breakup_leg(capi, device, pop, iterations, cfg_kw, min_altitude=150.0):
     t0 = time.perf_counter()
     with capi.Context(cfg) as ctx:
         ctx.upload(pop)
+        ctx.reserve(n + n // 8)  # room for fragments: appends reallocate nothing
         for it in range(iterations):
             if not ctx.integrate(1, allow_nonfinite=True):
                 tot["nonfinite_steps"] += 1
@@ -549,6 +550,7 @@ def applied_breakup_run(capi, cfg, bcfg, pop, iterations, min_altitude, wall_bud
     t0 = time.perf_counter()
     with capi.Context(cfg) as ctx:
         ctx.upload(pop)
+        ctx.reserve(n + n // 8)  # room for fragments: appends reallocate nothing
         try:
             for it in range(iterations):
                 t = [time.perf_counter()]

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define LADDS_GPU_ABI_VERSION 3
+#define LADDS_GPU_ABI_VERSION 4
 
 /* ---- status codes ---- */
 #define LADDS_OK 0
@@ -174,6 +174,13 @@ int ladds_gpu_upload(ladds_gpu_ctx *ctx, size_t n, const double *x, const double
 int ladds_gpu_append(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
                      const double *vx, const double *vy, const double *vz, const double *radius, const double *aom,
                      const double *bcInv, const uint64_t *id, const uint64_t *parentId, const int8_t *activity);
+/* Device capacity for at least `capacity` objects, so that appends up to it
+ * (breakup fragments, inserted satellites) reallocate nothing: a growth
+ * re-allocates every per-object buffer (~0.3 KB per object) and drops the
+ * captured graphs.  Never shrinks; the population is unchanged.  The
+ * counterpart of reserving the particle container before a run whose
+ * fragments are appended (Simulation.cpp:610-633, autopas addParticle). */
+int ladds_gpu_reserve(ladds_gpu_ctx *ctx, size_t capacity);
 /* Simulation::checkedInsert (Simulation.cpp:475-507): satellite i (arrays as
  * for ladds_gpu_append) is appended only if no particle of the population --
  * nor a satellite of this batch accepted before it -- lies in the half-open

@@ -90,7 +90,7 @@ EXPORTED = [
     "ladds_gpu_breakup", "ladds_gpu_select_layers", "ladds_gpu_layer_histogram", "ladds_gpu_remove_slots",
     "ladds_gpu_set_halo", "ladds_gpu_pack_layers", "ladds_gpu_append_records", "ladds_gpu_truncate",
     "ladds_gpu_step_host", "ladds_gpu_pending_records", "ladds_population_write",
-    "ladds_population_read",
+    "ladds_population_read", "ladds_gpu_reserve",
 ]
 
 STATE_RECORD_DTYPE = np.dtype([("r", "<f8", (3,)), ("v", "<f8", (3,)), ("radius", "<f8"), ("aom", "<f8"),
@@ -148,6 +148,7 @@ def lib():
     L.ladds_gpu_last_error.argtypes = [vp]
     L.ladds_gpu_upload.argtypes = [vp, sz] + [vp] * 12
     L.ladds_gpu_append.argtypes = [vp, sz] + [vp] * 12
+    L.ladds_gpu_reserve.argtypes = [vp, sz]
     L.ladds_gpu_download.argtypes = [vp, sz, C.POINTER(sz)] + [vp] * 12
     L.ladds_gpu_set_state.argtypes = [vp, sz] + [vp] * 6
     L.ladds_gpu_get_state.argtypes = [vp, sz] + [vp] * 6
@@ -295,6 +296,10 @@ class Context:
     def append(self, pop: dict):
         pop = as_population(pop)
         self._check(self._L.ladds_gpu_append(self._h, len(pop["x"]), *[_p(pop[k]) for k in POP_FIELDS]))
+
+    def reserve(self, capacity: int):
+        """Device capacity for at least `capacity` objects (appends up to it reallocate nothing)."""
+        self._check(self._L.ladds_gpu_reserve(self._h, int(capacity)))
 
     def size(self) -> int:
         n = C.c_size_t()

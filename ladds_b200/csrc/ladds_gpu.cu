@@ -1070,6 +1070,14 @@ int ladds_gpu_append(ladds_gpu_ctx *c, size_t n, const double *x, const double *
   return LADDS_OK;
 }
 
+int ladds_gpu_reserve(ladds_gpu_ctx *c, size_t capacity) {
+  if (!c) return LADDS_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_deviceMutex[c->dev & 63]);
+  if (capacity <= c->cap) return LADDS_OK;
+  CK(cudaSetDevice(c->dev));
+  return ensureCapacity(c, capacity);
+}
+
 int ladds_gpu_checked_insert(ladds_gpu_ctx *c, size_t n, const double *x, const double *y, const double *z,
                              const double *vx, const double *vy, const double *vz, const double *radius,
                              const double *aom, const double *bcInv, const uint64_t *id, const uint64_t *parentId,

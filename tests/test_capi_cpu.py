@@ -33,7 +33,7 @@ def test_exports_every_declared_symbol(capi):
     for name in names:
         assert hasattr(L, name), name
     assert set(names) == set(capi.EXPORTED)
-    assert L.ladds_gpu_abi_version() == 3
+    assert L.ladds_gpu_abi_version() == 4
 
 
 def test_config_layout_matches_header(capi):

@@ -485,6 +485,31 @@ def test_burnup_removal_and_append(capi):
     assert np.array_equal(back["id"], pop["id"]) and np.array_equal(back["x"], pop["x"])
 
 
+@pytest.mark.parametrize("reserve", [0, 7000])
+def test_reserve_then_append_steps_like_without(capi, reserve):
+    """ladds_gpu_reserve changes no result: with room reserved before the
+    append (no reallocation) the state and records after the append and two
+    steps equal those of a context that grew on the append."""
+    pop = capi.generate_population(0, 21, 5000)
+    extra = capi.generate_population(0, 22, 600)
+    extra["id"] = np.arange(20000, 20600, dtype=np.uint64)
+    outs = []
+    for res in (0, reserve):
+        with ctx_for(capi, useGraphs=1) as ctx:
+            ctx.upload(pop)
+            if res:
+                ctx.reserve(res)
+                ctx.reserve(10)  # never shrinks
+            r0 = ctx.step(3)
+            ctx.append(extra)
+            r1 = ctx.step(3)
+            outs.append((r0.records, r1.records, ctx.download()))
+    a, b = outs
+    assert records_equal(a[0], b[0]) and records_equal(a[1], b[1])
+    for k in ("x", "y", "z", "vx", "vy", "vz", "id"):
+        assert np.array_equal(a[2][k], b[2][k]), k
+
+
 def test_clear_parents(capi):
     pop = capi.generate_population(0, 8, 1000)
     pop["parent"][:] = 5
