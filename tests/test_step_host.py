@@ -1,7 +1,8 @@
 """ladds_gpu_step_host: one iteration with the positions and velocities in host
 memory, moved in chunks that are propagated while the next chunk crosses PCIe
-(pinned and pageable host arrays).  It must equal set_state + step(1) + get_state bit for bit: the state, the
-records, the cell order and the device copy of the population afterwards."""
+(pinned, pageable and mixed host arrays).  It must equal set_state + step(1) +
+get_state bit for bit: the state, the records, the cell order and the device
+copy of the population afterwards."""
 import numpy as np
 import pytest
 
@@ -166,3 +167,25 @@ def test_step_host_mixed_pinned_and_pageable(capi):
                 assert np.array_equal(x, y), f"state differs at iteration {it}"
             assert records_equal(ra.records, rb.records), describe_diff(ra.records, rb.records)
             host_in = out
+
+
+def test_step_host_pinned_in_pageable_out(capi):
+    """Pinned inputs with mostly pageable outputs (staged back through the
+    context's pinned buffer): same result."""
+    pop = capi.generate_population(0, 2033, 300_000)
+    kw = dict(componentMask=capi.PROP_ALL, precision=capi.PRECISION_SPLIT, conjunctionThreshold=10.0)
+    with capi.Context(capi.default_config(**kw)) as a, capi.Context(capi.default_config(**kw)) as b:
+        a.upload(pop)
+        b.upload(pop)
+        host = pinned_state([pop[f] for f in ("x", "y", "z", "vx", "vy", "vz")])
+        for it in range(2):
+            a.set_state(*host)
+            ra = a.step(1)
+            sa = a.get_state()
+            out = [np.zeros(len(h)) for h in host]
+            out[3] = pinned_state([out[3]])[0]  # one output array page-locked, the others pageable
+            rb = b.step_host(host, out)
+            for x, y in zip(sa, out):
+                assert np.array_equal(x, y), f"state differs at iteration {it}"
+            assert records_equal(ra.records, rb.records), describe_diff(ra.records, rb.records)
+            host = pinned_state(out)
