@@ -110,3 +110,37 @@ def test_objects_outside_the_box(capi, oracle):
     assert records_equal(ref, brute), describe_diff(ref, brute)
     assert len(ref) > 20
     assert records_equal(recs, ref), describe_diff(recs, ref)
+
+
+@pytest.mark.parametrize("box,cell", [(5.0e5, 0.0), (2.0e5, 2.0)])
+def test_coarsened_grid(capi, oracle, box, cell):
+    """A box too large for 32-bit cell keys at the requested edge (or for 65535
+    cells per axis): the grid is coarsened by 1.25x until it fits, identically
+    in the library and the oracle; cell order and records still match the
+    oracle and its brute force."""
+    rng = np.random.default_rng(11)
+    n = 4000
+    r = np.array([7000.0, 0.0, 0.0]) + rng.uniform(-150, 150, size=(n, 3))
+    v = rng.normal(size=(n, 3))
+    v *= rng.uniform(0.0, 5.0, size=(n, 1)) / np.linalg.norm(v, axis=1, keepdims=True)
+    pop = from_lists(r, v, np.arange(n), np.zeros(n, np.int8), np.full(n, 10.0), np.full(n, 1.0))
+    kw = dict(cutoff=10.0, cellSize=cell, collisionDistanceFactor=2000.0, evasionCutoff=3.0,
+              conjunctionThreshold=2.0, boxMin=[-box] * 3, boxMax=[box] * 3)
+    cfg = capi.default_config(**kw)
+    with capi.Context(cfg) as ctx:
+        ctx.upload(pop)
+        recs = ctx.conjunctions(10.0)
+        keys, slots = ctx.cell_order()
+        dims, reach, cell_used = ctx.grid()
+    grid = oracle.make_grid(kw["boxMin"], kw["boxMax"], cell, kw["cutoff"])
+    assert tuple(grid.n) == dims and grid.reach == reach and grid.cellSize == cell_used
+    assert cell_used > 10.0 and max(dims) <= 65535 and int(np.prod(dims, dtype=np.uint64)) <= 1 << 32
+    opop = to_oracle(oracle, pop)
+    p = oracle_params(oracle, cfg, 10.0)
+    ref = oracle.scan_cells(opop, p, grid)
+    assert len(ref) > 0
+    assert records_equal(recs, ref), describe_diff(recs, ref)
+    assert records_equal(ref, oracle.scan_bruteforce(opop, p))
+    okeys = oracle.cell_keys(opop, grid)
+    operm = oracle.stable_sort(okeys)
+    assert np.array_equal(slots, operm) and np.array_equal(keys, okeys[operm])
