@@ -13,8 +13,9 @@ figure and their ratio are reported beside it, and further legs measure:
 split vs FP64 per population (position drift and the conjunction sets compared
 pair by pair), the constellation and 8e6 scale populations (autotuned), the
 adjoint of 4096 conjunction pairs with its finite-difference check, and the 8e6
-population's breakups over one day.  The line ends with ``north_star``, a
-summary of those figures.  ``e2e`` runs the same steps through the C ABI in the host-owned
+population's breakups over one day.  The line ends with ``targets``, a
+summary of those figures against the targets (mixed / FP64, drift, conjunction
+sets, adjoint / forward, finite-difference agreement, breakup counts).  ``e2e`` runs the same steps through the C ABI in the host-owned
 mode of the drop-in (ladds_gpu_step_host): per step the positions/velocities
 go host->device from pinned memory, the step runs, positions/velocities and
 the conjunction records come back; ``e2e.device_resident`` is the drop-in's own data flow, the
@@ -967,7 +968,7 @@ def main():
     # cannot exceed the FP64 step over its non-propagation part
     fp64_per = {k: fp64_ph[k] / fp64_ph["steps"] for k in capi.PhaseTimes.PHASES}
     shared_ms = max(sum(fp64_per.values()) - fp64_per["propagate"], 1e-9)
-    north = {
+    targets = {
         "mixed_over_fp64": value / fp64_value,
         "fp64_value": fp64_value,
         "propagate_fp64_over_split": fp64_per["propagate"] / max(per["propagate"], 1e-12),
@@ -1017,7 +1018,7 @@ def main():
         "clocks": split["clocks"],
         "gpu_launches": int(round(launches_per_step * args.steps)) + (args.steps + 127) // 128,
         "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / args.steps},
-        "north_star": north,
+        "targets": targets,
     }
     print(json.dumps(line), flush=True)
     if world > 1:
