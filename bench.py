@@ -795,8 +795,11 @@ def main():
         ctx.set_profiling(False)
         ctx.close()
 
+    # the characterisation legs run once, in the one-GPU run: with replicas on
+    # several GPUs they would hold every GPU while rank 0 alone works
+    legs = world == 1
     workloads = {}
-    if not args.no_workloads and rank == 0:
+    if not args.no_workloads and legs:
         for name, which, n_obj, steps, tune in (("constellation_shells", 2, 2_004_224, 128, True),
                                                 ("scale_8M", 4, 8_000_000, 32, True)):
             try:
@@ -805,7 +808,7 @@ def main():
                 workloads[name] = {"error": str(ex)[:200]}
 
     adjoint = None
-    if not args.no_adjoint and rank == 0:
+    if not args.no_adjoint and legs:
         try:
             adjoint = adjoint_leg(capi, local)
         except Exception as ex:  # noqa: BLE001
@@ -820,7 +823,7 @@ def main():
     tuned = workloads.get("scale_8M", {}).get("autotuned")
     if tuned:
         scale_kw = {k: tuned[k] for k in ("cellSize", "scanScreen", "walkForm", "propagateBlock", "scanBlock")}
-    if not args.no_drift and rank == 0:
+    if not args.no_drift and legs:
         for name, mk_pop, steps, kw in (
                 ("population0_1e6", lambda: pop, STEPS_PER_DAY, {}),
                 ("constellation_shells_2e6", lambda: capi.generate_population(2, SEED + 2, 2_004_224),
@@ -836,7 +839,7 @@ def main():
                 print(f"drift leg {name} failed: {ex}", file=sys.stderr)
 
     breakups = None
-    if not args.no_workloads and rank == 0 and args.breakup_steps > 0:
+    if not args.no_workloads and legs and args.breakup_steps > 0:
         try:
             breakups = breakup_leg(capi, local, capi.generate_population(4, SEED + 4, 8_000_000),
                                    args.breakup_steps, scale_kw)
@@ -987,6 +990,7 @@ def main():
                                                                               "stopped_by")}}
                          if breakups and "error" not in breakups else breakups),
         "value_over_cpu_baseline": value / cpu["value"] if cpu and cpu.get("value") else None,
+        "legs": "this run" if legs else "reported by the one-GPU run (replicas: timed steps and e2e only)",
     }
     line = {
         "metric": METRIC,
