@@ -884,6 +884,19 @@ def main():
         el = dist_max(time.perf_counter() - t0, world)
         e2e["three_calls"] = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
                               "mode": "set_state / step(1) / get_state per iteration, pinned"}
+        # the same with pageable arrays (a std::vector's storage: ladds::Integrator without residency)
+        pageable = [np.array(a) for a in pinned]
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ctx.set_state(*pageable)
+            ctx.step(1, out=out)
+            ctx._check(ctx._L.ladds_gpu_get_state(ctx.handle, n, *[a.ctypes.data_as(capi.C.c_void_p)
+                                                                    for a in pageable]))
+        el = dist_max(time.perf_counter() - t0, world)
+        e2e["three_calls_pageable"] = {"value": world * n * args.e2e_steps / el, "unit": "object-steps/s",
+                                       "mode": "set_state / step(1) / get_state per iteration, pageable "
+                                               "(staged through the context's pinned buffer)"}
         # the drop-in's own data flow (ladds::HotPathLoop): the population stays on the device and
         # each iteration's records come back to the host (pinned) from one ladds_gpu_step(1) call
         outp = torch.empty((1 << 16) * capi.PAIR_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True).numpy()

@@ -198,7 +198,11 @@ int ladds_gpu_download(ladds_gpu_ctx *ctx, size_t cap, size_t *n, double *x, dou
                        double *vy, double *vz, double *radius, double *aom, double *bcInv, uint64_t *id,
                        uint64_t *parentId, int8_t *activity);
 /* Uploads / downloads only positions and velocities, in slot order (the
- * host-owned-container mode of the drop-in). */
+ * host-owned-container mode of the drop-in).  Pageable arrays (a
+ * std::vector's storage) go through the context's pinned staging buffer,
+ * copied on all host threads while the previous array crosses PCIe (the
+ * buffer of ladds_gpu_step_host, 96 B per object, allocated on first use);
+ * pinned arrays are copied directly. */
 int ladds_gpu_set_state(ladds_gpu_ctx *ctx, size_t n, const double *x, const double *y, const double *z,
                         const double *vx, const double *vy, const double *vz);
 int ladds_gpu_get_state(ladds_gpu_ctx *ctx, size_t n, double *x, double *y, double *z, double *vx, double *vy,

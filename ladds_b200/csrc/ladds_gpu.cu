@@ -867,6 +867,53 @@ int allocGridBuffers(ladds_gpu_ctx *c) {
   return LADDS_OK;
 }
 
+constexpr size_t kHostCopyBlock = (size_t)1 << 17;  // doubles per task of the staging copies
+
+bool isPinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// dst[a][lo, lo + len) = src[a][lo, lo + len) for the arrays with use[a], on all host threads
+void hostCopy(double *const dst[6], const double *const src[6], const bool use[6], size_t lo, size_t len) {
+  const long per = (long)((len + kHostCopyBlock - 1) / kHostCopyBlock);
+#pragma omp parallel for schedule(static)
+  for (long t = 0; t < 6 * per; ++t) {
+    const int a = (int)(t / per);
+    if (!use[a]) continue;
+    const size_t b = lo + (size_t)(t % per) * kHostCopyBlock, e = std::min(b + kHostCopyBlock, lo + len);
+    std::memcpy(dst[a] + b, src[a] + b, (e - b) * sizeof(double));
+  }
+}
+
+// dst[0, n) = src[0, n) on all host threads
+void hostCopyOne(double *dst, const double *src, size_t n) {
+  const double *const s6[6] = {src, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double *const d6[6] = {dst, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const bool use[6] = {true, false, false, false, false, false};
+  hostCopy(d6, s6, use, 0, n);
+}
+
+// the context's pinned staging buffer for pageable host arrays: 12 arrays of
+// at least n doubles (six in, six out); false if no pinned memory is to be had
+// (the CUDA driver then stages the copies itself)
+bool ensurePinStage(ladds_gpu_ctx *c, size_t n) {
+  if (c->pinStage && c->pinCap >= n) return true;
+  if (c->pinStage) cudaFreeHost(c->pinStage);
+  c->pinStage = nullptr;
+  c->pinCap = 0;
+  if (cudaHostAlloc(&c->pinStage, 12 * n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    c->pinStage = nullptr;
+    return false;
+  }
+  c->pinCap = n;
+  return true;
+}
 }  // namespace
 
 extern "C" {
@@ -1238,10 +1285,25 @@ int ladds_gpu_set_state(ladds_gpu_ctx *c, size_t n, const double *x, const doubl
   double *dst[] = {c->cur.x, c->cur.y, c->cur.z, c->cur.vx, c->cur.vy, c->cur.vz};
   double *stage[] = {c->alt.x, c->alt.y, c->alt.z, c->alt.vx, c->alt.vy, c->alt.vz};
   const int g = blocksFor(n, 256);
+  // pageable arrays go through the context's pinned staging, copied on all host
+  // threads while the previous array crosses PCIe
+  bool pinned[6], staged = false;
+  for (int k = 0; k < 6; ++k) {
+    pinned[k] = isPinned(src[k]);
+    staged |= !pinned[k];
+  }
+  if (staged && !ensurePinStage(c, n))
+    for (bool &p : pinned) p = true;  // no pinned memory to spare: the driver stages them
   // the copies run back to back on the main stream; each array's gather into
   // cell order runs on the second stream while the next array crosses PCIe
   for (int k = 0; k < 6; ++k) {
-    CK(cudaMemcpyAsync(stage[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    const double *from = src[k];
+    if (!pinned[k]) {
+      double *pin = c->pinStage + (size_t)k * c->pinCap;
+      hostCopyOne(pin, src[k], n);
+      from = pin;
+    }
+    CK(cudaMemcpyAsync(stage[k], from, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(cudaEventRecord(c->evXfer[k], c->st));
     CK(cudaStreamWaitEvent(c->st2, c->evXfer[k], 0));
     k_permute_from_slots_f64<<<g, 256, 0, c->st2>>>(stage[k], c->cur.tag, (int)n, dst[k]);
@@ -1272,10 +1334,26 @@ int ladds_gpu_get_state(ladds_gpu_ctx *c, size_t n, double *x, double *y, double
     k_unpermute_f64<<<g, 256, 0, c->st2>>>(src[k], c->cur.tag, (int)c->n, stage[k]);
     CK(cudaEventRecord(c->evXfer[k], c->st2));
   }
+  // pageable arrays come back through the context's pinned staging: each
+  // array leaves the pinned buffer on all host threads while the next crosses PCIe
+  bool pinned[6], staged = false;
+  for (int k = 0; k < 6; ++k) {
+    pinned[k] = !dst[k] || isPinned(dst[k]);
+    staged |= !pinned[k];
+  }
+  if (staged && !ensurePinStage(c, c->n))
+    for (bool &p : pinned) p = true;  // no pinned memory to spare: the driver stages them
   for (int k = 0; k < 6; ++k) {
     if (!dst[k]) continue;
     CK(cudaStreamWaitEvent(c->st, c->evXfer[k], 0));
-    CK(cudaMemcpyAsync(dst[k], stage[k], c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    double *to = pinned[k] ? dst[k] : c->pinStage + (size_t)(6 + k) * c->pinCap;
+    CK(cudaMemcpyAsync(to, stage[k], c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaEventRecord(c->evPipe[k], c->st));
+  }
+  for (int k = 0; k < 6; ++k) {
+    if (!dst[k] || pinned[k]) continue;
+    CK(cudaEventSynchronize(c->evPipe[k]));
+    hostCopyOne(dst[k], c->pinStage + (size_t)(6 + k) * c->pinCap, c->n);
   }
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
@@ -1601,30 +1679,6 @@ int ladds_gpu_step(ladds_gpu_ctx *c, int iterations, ladds_pair *out, size_t cap
 
 }  // extern "C"
 
-namespace {
-constexpr size_t kHostCopyBlock = (size_t)1 << 17;  // doubles per task of the staging copies
-
-bool isPinned(const void *p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
-// dst[a][lo, lo + len) = src[a][lo, lo + len) for the arrays with use[a], on all host threads
-void hostCopy(double *const dst[6], const double *const src[6], const bool use[6], size_t lo, size_t len) {
-  const long per = (long)((len + kHostCopyBlock - 1) / kHostCopyBlock);
-#pragma omp parallel for schedule(static)
-  for (long t = 0; t < 6 * per; ++t) {
-    const int a = (int)(t / per);
-    if (!use[a]) continue;
-    const size_t b = lo + (size_t)(t % per) * kHostCopyBlock, e = std::min(b + kHostCopyBlock, lo + len);
-    std::memcpy(dst[a] + b, src[a] + b, (e - b) * sizeof(double));
-  }
-}
-}  // namespace
 
 extern "C" {
 
@@ -1685,18 +1739,9 @@ int ladds_gpu_step_host(ladds_gpu_ctx *c, size_t n, const double *const in[6], d
     anyIn |= stageIn[a];
     anyOut |= stageOut[a];
   }
-  if ((anyIn || anyOut) && c->pinCap < n) {
-    if (c->pinStage) cudaFreeHost(c->pinStage);
-    c->pinStage = nullptr;
-    c->pinCap = 0;
-    if (cudaHostAlloc(&c->pinStage, 12 * n * sizeof(double), cudaHostAllocDefault) == cudaSuccess) {
-      c->pinCap = n;
-    } else {  // no pinned memory to spare: the CUDA driver stages the copies
-      cudaGetLastError();
-      c->pinStage = nullptr;
-      for (int a = 0; a < 6; ++a) stageIn[a] = stageOut[a] = false;
-      anyIn = anyOut = false;
-    }
+  if ((anyIn || anyOut) && !ensurePinStage(c, n)) {  // no pinned memory to spare: the driver stages the copies
+    for (int a = 0; a < 6; ++a) stageIn[a] = stageOut[a] = false;
+    anyIn = anyOut = false;
   }
   double *pinIn[6], *pinOut[6];
   const double *src[6];
