@@ -46,7 +46,7 @@ struct DenseBin {
   uint32_t *chunk;
 };
 constexpr uint32_t kDenseCell = 12;   // objects per cell from which the cell is scanned by tiles
-constexpr uint32_t kTileChunk = 256;  // source objects of one dense-bin work item
+constexpr uint32_t kTileChunk = 64;  // source objects of one dense-bin work item
 
 __device__ __forceinline__ void denseAppend(const DenseBin &d, uint32_t key, uint32_t objects) {
   const uint32_t nch = (objects + kTileChunk - 1) / kTileChunk;
