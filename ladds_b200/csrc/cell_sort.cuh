@@ -35,9 +35,12 @@ constexpr int kBucketThreads = 256;
 // listed (key r * nx + ix) by the row sorts; their objects are scanned by cell
 // tiles (k_pair_tiles) instead of the per-object walk.  cells == nullptr: off.
 // A cell of more than kTileChunk objects is listed once per chunk of
-// kTileChunk source objects (cells[q], chunk[q] = chunk index), so that the
-// objects of a crowded cell -- a breakup's fragments start at one point -- are
-// shared out over many warps.
+// kTileChunk source objects, and a crowded cell once more per part of its
+// staged neighbours: entry (cells[q], chunk[q] = chunk index | part << 24 |
+// log2(parts) << 28) tests its chunk's sources against the staged blocks
+// part, part + parts, ... of the cell's half shell.  So the objects of a
+// crowded cell -- a breakup's fragments start at one point, and its
+// neighbours are crowded too -- are shared out over many warps on both sides.
 struct DenseBin {
   uint32_t *cells;
   uint32_t *count;
@@ -48,13 +51,26 @@ struct DenseBin {
 constexpr uint32_t kDenseCell = 12;   // objects per cell from which the cell is scanned by tiles
 constexpr uint32_t kTileChunk = 64;  // source objects of one dense-bin work item
 
+constexpr uint32_t kTilePartsLogMax = 4;  // up to 16 parts of the staged side
+
+// log2 of the parts the staged side of a cell of `objects` objects is split into
+__host__ __device__ __forceinline__ uint32_t tilePartsLog(uint32_t objects) {
+  uint32_t lp = 0;
+  while (lp < kTilePartsLogMax && objects >= (64u << (2 * lp))) ++lp;
+  return lp;
+}
+
 __device__ __forceinline__ void denseAppend(const DenseBin &d, uint32_t key, uint32_t objects) {
   const uint32_t nch = (objects + kTileChunk - 1) / kTileChunk;
-  const uint32_t q = atomicAdd(d.count, nch);
+  const uint32_t lp = tilePartsLog(objects), parts = 1u << lp;
+  const uint32_t q = atomicAdd(d.count, nch * parts);
   for (uint32_t ch = 0; ch < nch; ++ch)
-    if (q + ch < d.cap) {
-      d.cells[q + ch] = key;
-      d.chunk[q + ch] = ch;
+    for (uint32_t pt = 0; pt < parts; ++pt) {
+      const uint32_t e = q + ch * parts + pt;
+      if (e < d.cap) {
+        d.cells[e] = key;
+        d.chunk[e] = ch | (pt << 24) | (lp << 28);
+      }
     }
 }
 

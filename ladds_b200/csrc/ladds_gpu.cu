@@ -306,8 +306,9 @@ int ensureCapacity(ladds_gpu_ctx *c, size_t need) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
-  // every listed cell holds >= kDenseCell objects and adds one entry per kTileChunk of them
-  c->denseCap = (uint32_t)(newCap / kDenseCell + newCap / kTileChunk + 1);
+  // every listed cell holds >= kDenseCell objects and adds one entry per kTileChunk of them and part of
+  // its staged side (up to 2^kTilePartsLogMax parts, for cells of >= 64 * 4^kTilePartsLogMax objects)
+  c->denseCap = (uint32_t)(newCap / kDenseCell + newCap / kTileChunk * (1u << kTilePartsLogMax) + 1);
   for (uint32_t **p : {&c->denseCells, &c->denseCellsB, &c->denseChunk, &c->denseChunkB}) {
     if (cudaMalloc(p, (size_t)c->denseCap * sizeof(uint32_t)) != cudaSuccess) {
       cudaGetLastError();

@@ -635,7 +635,9 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
                   iz = (int32_t)(r / (uint32_t)ny);
     uint32_t c0, c1;  // the cell's objects
     rowWindow(r, (uint32_t)ix, (uint32_t)ix, (uint32_t)nx, rowStart, cellOff, skeys, c0, c1);
-    const uint32_t s0 = c0 + denseChunk[q] * kTileChunk, s1 = min(c1, s0 + kTileChunk);  // this entry's sources
+    const uint32_t cw = denseChunk[q];  // chunk | part << 24 | log2(parts) << 28
+    const uint32_t part = (cw >> 24) & 15u, partsLog = cw >> 28;
+    const uint32_t s0 = c0 + (cw & 0xffffffu) * kTileChunk, s1 = min(c1, s0 + kTileChunk);  // this entry's sources
     // lane q: window of half-shell row q
     uint32_t lo = 0, hi = 0;
     if (lane < nq) {
@@ -659,7 +661,7 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     const uint32_t excl = incl - cnt;
     const uint32_t ownEnd = __shfl_sync(0xffffffffu, incl, 0);  // staged items [0, ownEnd) are own-row objects
-    for (uint32_t stBase = 0; stBase < total; stBase += kTileStage) {
+    for (uint32_t stBase = part * kTileStage; stBase < total; stBase += kTileStage << partsLog) {  // this part's blocks
       const uint32_t m = min(kTileStage, total - stBase);
       bool oneGroup = grp != nullptr;  // every staged object in one breakup group (warp-uniform after the loop)
       uint32_t g0 = kNoGroup;
