@@ -52,6 +52,7 @@ constexpr uint32_t kDenseCell = 12;   // objects per cell from which the cell is
 constexpr uint32_t kTileChunk = 64;  // source objects of one dense-bin work item
 
 constexpr uint32_t kTilePartsLogMax = 4;  // up to 16 parts of the staged side
+static_assert((1u << kTilePartsLogMax) <= 16u, "the part index of a dense-bin entry has 4 bits");
 
 // log2 of the parts the staged side of a cell of `objects` objects is split into
 __host__ __device__ __forceinline__ uint32_t tilePartsLog(uint32_t objects) {
