@@ -498,9 +498,9 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
       }
     }
     __syncthreads();
-    for (uint32_t k = 2; k <= P; k <<= 1) {
-      for (uint32_t jj = k / 2; jj > 0; jj >>= 1) {
-        if (inShared) {
+    if (inShared) {
+      for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t jj = k / 2; jj > 0; jj >>= 1) {
           for (uint32_t i = threadIdx.x; i < P / 2; i += blockDim.x) {
             uint32_t lo, hi;
             bitonicPair(i, k, jj, lo, hi);
@@ -515,10 +515,60 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
               }
             }
           }
-        } else {
-          // in global memory (beyond kLargeRow objects: a breakup's fragment
-          // cloud): the comparators of a stage touch disjoint pairs, so each
-          // thread loads four pairs before it compares any (four loads in flight)
+          __syncthreads();
+        }
+      }
+    } else {
+      // in global memory (beyond kLargeRow objects: a breakup's fragment
+      // cloud).  Every stage whose comparators stay inside aligned blocks of
+      // kLargeRow elements runs block by block in shared memory: first the
+      // whole network up to k = kLargeRow, then, for each larger k, its stages
+      // jj < kLargeRow after the global ones (jj >= kLargeRow).  Comparator i of
+      // block b is comparator b * kLargeRow / 2 + i of the row.
+      const uint32_t nBlocks = P / (uint32_t)kLargeRow;
+      // stages (kk, jj) for kk = kFirst .. kLast (doubling), jj from jjFirst (for
+      // kk = kFirst; kk / 2 after) down to 1, block by block in shared memory
+      auto blockStages = [&](uint32_t kFirst, uint32_t kLast, uint32_t jjFirst) {
+        for (uint32_t bl = 0; bl < nBlocks; ++bl) {
+          const uint32_t base = bl * (uint32_t)kLargeRow;
+          if (base >= L) break;  // blocks of padding only: nothing to compare
+          const uint32_t n = min((uint32_t)kLargeRow, L - base);
+          for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            sv[i] = V[base + i];
+            sp[i] = I[base + i];
+          }
+          __syncthreads();
+          for (uint32_t kk = kFirst; kk <= kLast; kk <<= 1) {
+            for (uint32_t jj = kk == kFirst ? jjFirst : kk / 2; jj > 0; jj >>= 1) {
+              for (uint32_t i = threadIdx.x; i < (uint32_t)kLargeRow / 2; i += blockDim.x) {
+                uint32_t lo, hi;
+                bitonicPair(i, kk, jj, lo, hi);
+                if (hi < n) {
+                  const unsigned long long x = sv[lo], y = sv[hi];
+                  if (y < x) {
+                    sv[lo] = y;
+                    sv[hi] = x;
+                    const uint32_t t = sp[lo];
+                    sp[lo] = sp[hi];
+                    sp[hi] = t;
+                  }
+                }
+              }
+              __syncthreads();
+            }
+          }
+          for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            V[base + i] = sv[i];
+            I[base + i] = sp[i];
+          }
+          __syncthreads();
+        }
+      };
+      blockStages(2u, (uint32_t)kLargeRow, 1u);  // each block sorted
+      for (uint32_t k = 2u * (uint32_t)kLargeRow; k <= P; k <<= 1) {
+        for (uint32_t jj = k / 2; jj >= (uint32_t)kLargeRow; jj >>= 1) {
+          // the comparators of a stage touch disjoint pairs, so each thread
+          // loads four pairs before it compares any (four loads in flight)
           for (uint32_t i0 = threadIdx.x; i0 < P / 2; i0 += 4u * blockDim.x) {
             uint32_t lo[4], hi[4];
             unsigned long long a[4], b[4];
@@ -547,8 +597,9 @@ __global__ void __launch_bounds__(kBucketThreads) k_bucket_sort_large(
               }
             }
           }
+          __syncthreads();
         }
-        __syncthreads();
+        blockStages(k, k, (uint32_t)kLargeRow / 2);
       }
     }
     for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
