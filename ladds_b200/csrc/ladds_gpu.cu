@@ -628,7 +628,8 @@ void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, flo
   const DenseBin dense = denseBin(c);
   {
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
-    cudaMemsetAsync(c->dCandCount, 0, 2 * sizeof(unsigned long long), s);
+    // the two list lengths and the dense bin's next-entry counter
+    cudaMemsetAsync(c->dCandCount, 0, 3 * sizeof(unsigned long long), s);
     const CandSink out{sc,       c->posf,     c->velf,      c->dCand, c->dCandCount, (unsigned long long)c->candCap,
                        c->haloStart, c->anyParent ? c->grp : nullptr};
     const bool buffer = c->cfg.scanScreen == LADDS_SCREEN_BUFFER;
@@ -1001,7 +1002,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
       cudaMalloc(&c->denseCount, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->denseCountB, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&c->dCount, 3 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&c->dCandCount, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->dCandCount, 3 * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dEph, 3 * kMaxEphSteps * sizeof(EphEntry)) != cudaSuccess ||
       cudaMalloc(&c->dIter, 2 * sizeof(int64_t)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1022,7 +1023,7 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaEventCreateWithFlags(&c->evScan, cudaEventDisableTiming);
   for (auto &e : c->evXfer) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto &e : c->evPipe) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
-  cudaMemset(c->dCandCount, 0, 2 * sizeof(unsigned long long));
+  cudaMemset(c->dCandCount, 0, 3 * sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);

@@ -624,11 +624,19 @@ __global__ void __launch_bounds__(kScanCta) k_pair_tiles(const uint32_t *__restr
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t nBuf = 0;  // pairs in this warp's buffer (warp-uniform)
   const uint32_t nDense = min(*denseCount, denseCap);
-  const uint32_t gw = (blockIdx.x * kScanCta + threadIdx.x) >> 5, nW = (gridDim.x * kScanCta) >> 5;
   const int32_t nx = g.n[0], ny = g.n[1], nz = g.n[2], R = g.reach;
   const int nq = (R + 1) + R * (2 * R + 1);  // half-shell rows (<= 32 for R <= 3)
   const uint32_t *grp = out.grp;
-  for (uint32_t q = gw; q < nDense; q += nW) {
+  // entries are handed out one at a time (out.count[2], zeroed with the list
+  // lengths before the scan), so a warp that drew a long entry -- a crowded
+  // cell's -- does not hold back entries that were dealt to it in advance
+  unsigned long long *next = out.count + 2;
+  for (;;) {
+    if (nDense == 0u) break;  // an empty bin (the common case) costs no atomics
+    uint32_t q = 0;
+    if (lane == 0) q = (uint32_t)min(atomicAdd(next, 1ull), (unsigned long long)nDense);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= nDense) break;
     const uint32_t key = denseCells[q];
     const uint32_t r = key / (uint32_t)nx;
     const int32_t ix = (int32_t)(key - r * (uint32_t)nx), iy = (int32_t)(r % (uint32_t)ny),
