@@ -9,9 +9,10 @@
 // both initial states and dL/dbcInv of both objects (bcInv = Cd A / m enters
 // the drag term).
 //
-// Forward (k_adj_forward): one thread per object, the two objects of a pair
-// in adjacent lanes (states exchanged by shuffles after every step); the
-// state is stored every `ck` steps (checkpoints).
+// Forward (k_adj_forward): one lane per object in each of kAdjWarps warps
+// that share out its force terms, the two objects of a pair in adjacent lanes
+// (states exchanged by shuffles after every step); the state is stored every
+// `ck` steps (checkpoints).
 // Backward (k_adj_backward): segments of ck steps in reverse order; each is
 // recomputed from its checkpoint, storing per step the start state and the
 // three stage accelerations (15 doubles), then swept in reverse:
@@ -190,13 +191,102 @@ __device__ __forceinline__ void adjStep(uint32_t mask, double r[3], double v[3],
   for (int k = 0; k < 3; ++k) r[k] += pc.hc1 * v[k];
 }
 
-// Reverse of one step: (r0, v0) = the step's start state, acc its stage
+// The forward and backward kernels run kAdjWarps warps per block over the
+// same 32 objects (lane = object) and share the force terms out among the
+// warps (balanced by their FP64 instruction counts): every warp holds the
+// whole state, evaluates its terms, and the partial accelerations (or
+// transposed-Jacobian products) meet in shared memory, where every warp adds
+// them in warp order -- the same sum in every warp.  The dependent chain of a
+// step, not the instruction total, bounds these kernels (a few thousand
+// objects), so a quarter of the terms per warp is a shorter step; the terms
+// go to whole warps, not to lanes of one warp, which would run them one after
+// another.  One block barrier per stage; the exchange buffer alternates
+// between two halves, so a warp that has passed the barrier of stage n + 1
+// cannot overwrite the half that a slower warp still reads for stage n.
+constexpr int kAdjWarps = 4;
+constexpr int kAdjObjs = 32;  // objects per block
+__device__ __forceinline__ uint32_t adjWarpTerms(uint32_t w) {
+  switch (w & 3u) {
+    case 0: return kPropKEP | kPropJ2;
+    case 1: return kPropDRAG;
+    case 2: return kPropJ3 | kPropC22 | kPropS22 | kPropSRP;
+    default: return kPropSOL | kPropLUN;
+  }
+}
+static_assert(kAdjWarps == 4, "adjWarpTerms shares the terms out over four warps");
+
+// exchange buffer: [half][warp][value][lane]
+template <int V>
+struct AdjExchange {
+  double x[2][kAdjWarps][V][kAdjObjs];
+};
+
+// sums x[0..V) over the block's warps (in warp order) into x; flips `half`
+template <int V, int N>
+__device__ __forceinline__ void warpTermSum(AdjExchange<N> &ex, int &half, double (&x)[V]) {
+  static_assert(V <= N, "exchange buffer too small");
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < V; ++k) ex.x[half][w][k][lane] = x[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    double t = ex.x[half][0][k][lane];
+#pragma unroll
+    for (int q = 1; q < kAdjWarps; ++q) t += ex.x[half][q][k][lane];
+    x[k] = t;
+  }
+  half ^= 1;
+}
+
+// adjStep with the terms shared out over the block's warps
+template <int N>
+__device__ __forceinline__ void adjStepWarps(AdjExchange<N> &ex, int &half, uint32_t mask, double r[3],
+                                             double v[3], double aom, double bc, const EphEntry *e3,
+                                             const AtmShared &atm, const PropConsts &pc, double acc[3][3]) {
+  const uint32_t mine = mask & adjWarpTerms(threadIdx.x >> 5);
+  const double hc[3] = {pc.hc1, pc.hc2, pc.hc2}, hd[3] = {pc.hd1, pc.hd2, pc.hd1};
+#pragma unroll
+  for (int st = 0; st < 3; ++st) {
+    double a[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] += hc[st] * v[k];
+    accel<false>(mine, r, v, aom, bc, e3[st], atm, a);
+    warpTermSum(ex, half, a);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      acc[st][k] = a[k];
+      v[k] += hd[st] * a[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) r[k] += pc.hc1 * v[k];
+}
+
+// accelVjp with the terms shared out over the block's warps, summed into lr, lv, lbc
+__device__ __forceinline__ void accelVjpWarps(AdjExchange<7> &ex, int &half, uint32_t mask, const double r[3],
+                                              const double v[3], double aom, double bc, const EphEntry &e,
+                                              const AtmShared &atm, const double g[3], double lr[3],
+                                              double lv[3], double &lbc) {
+  double t[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  accelVjp(mask & adjWarpTerms(threadIdx.x >> 5), r, v, aom, bc, e, atm, g, t, t + 3, t[6]);
+  warpTermSum(ex, half, t);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lr[k] += t[k];
+    lv[k] += t[3 + k];
+  }
+  lbc += t[6];
+}
+
+// Reverse of one step, the terms shared out over the block's warps: (r0, v0) = the step's start state, acc its stage
 // accelerations; (lr, lv, lbc) enter as the adjoint of the step's end state.
-__device__ __forceinline__ void adjReverseStep(uint32_t mask, const double r0[3], const double v0[3],
-                                               const double acc[3][3], double aom, double bc, const EphEntry *e3,
-                                               const AtmShared &atm, const PropConsts &pc, double lr[3],
-                                               double lv[3], double &lbc) {
-  // stage states, with the forward's own operations
+__device__ __forceinline__ void adjReverseStepWarps(AdjExchange<7> &ex, int &half, uint32_t mask,
+                                                    const double r0[3], const double v0[3],
+                                                    const double acc[3][3], double aom, double bc,
+                                                    const EphEntry *e3, const AtmShared &atm,
+                                                    const PropConsts &pc, double lr[3], double lv[3],
+                                                    double &lbc) {
   double r1[3], v1[3], r2[3], v2[3], r3[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -213,22 +303,22 @@ __device__ __forceinline__ void adjReverseStep(uint32_t mask, const double r0[3]
   }
   double g[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) lv[k] += pc.hc1 * lr[k];  // r4 = r3 + c1 h v3
+  for (int k = 0; k < 3; ++k) lv[k] += pc.hc1 * lr[k];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) g[k] = pc.hd1 * lv[k];  // v3 = v2 + d1 h a(r3, v2)
-  accelVjp(mask, r3, v2, aom, bc, e3[2], atm, g, lr, lv, lbc);
+  for (int k = 0; k < 3; ++k) g[k] = pc.hd1 * lv[k];
+  accelVjpWarps(ex, half, mask, r3, v2, aom, bc, e3[2], atm, g, lr, lv, lbc);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) lv[k] += pc.hc2 * lr[k];  // r3 = r2 + c2 h v2
+  for (int k = 0; k < 3; ++k) lv[k] += pc.hc2 * lr[k];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) g[k] = pc.hd2 * lv[k];  // v2 = v1 + d2 h a(r2, v1)
-  accelVjp(mask, r2, v1, aom, bc, e3[1], atm, g, lr, lv, lbc);
+  for (int k = 0; k < 3; ++k) g[k] = pc.hd2 * lv[k];
+  accelVjpWarps(ex, half, mask, r2, v1, aom, bc, e3[1], atm, g, lr, lv, lbc);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) lv[k] += pc.hc2 * lr[k];  // r2 = r1 + c2 h v1
+  for (int k = 0; k < 3; ++k) lv[k] += pc.hc2 * lr[k];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) g[k] = pc.hd1 * lv[k];  // v1 = v0 + d1 h a(r1, v0)
-  accelVjp(mask, r1, v0, aom, bc, e3[0], atm, g, lr, lv, lbc);
+  for (int k = 0; k < 3; ++k) g[k] = pc.hd1 * lv[k];
+  accelVjpWarps(ex, half, mask, r1, v0, aom, bc, e3[0], atm, g, lr, lv, lbc);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) lv[k] += pc.hc1 * lr[k];  // r1 = r0 + c1 h v0
+  for (int k = 0; k < 3; ++k) lv[k] += pc.hc1 * lr[k];
 }
 
 // Squared miss distance of the pair (i = A, j = B) over the step just ended
@@ -249,27 +339,31 @@ __device__ __forceinline__ double shflPartner(unsigned m, double x) { return __s
 
 // Object SoA: st[c * nObj + j], c = x, y, z, vx, vy, vz; objects 2p (A) and
 // 2p + 1 (B) form pair p.  Checkpoint k (state after step k * ck) at
-// ckpt[(k * 6 + c) * nObj + j], k = 0 .. (S - 1) / ck.
-__global__ void __launch_bounds__(128) k_adj_forward(const double *__restrict__ st, const double *__restrict__ bc,
-                                                     const double *__restrict__ aom, int nObj, int steps, int ck,
-                                                     const EphEntry *__restrict__ eph, PropConsts pc, double dt,
-                                                     double *__restrict__ ckpt, double *__restrict__ miss,
-                                                     int *__restrict__ argStep) {
+// ckpt[(k * 6 + c) * nObj + j], k = 0 .. (S - 1) / ck.  Blocks of kAdjWarps
+// warps over kAdjObjs objects (lane = object, both objects of a pair in
+// adjacent lanes); warp 0 writes.  Lanes past the last object step a copy of
+// it (every warp reaches every block barrier) and write nothing.
+__global__ void __launch_bounds__(kAdjWarps * 32) k_adj_forward(
+    const double *__restrict__ st, const double *__restrict__ bc, const double *__restrict__ aom, int nObj,
+    int steps, int ck, const EphEntry *__restrict__ eph, PropConsts pc, double dt, double *__restrict__ ckpt,
+    double *__restrict__ miss, int *__restrict__ argStep) {
   __shared__ AtmShared atm;
+  __shared__ AdjExchange<3> ex;
   loadAtm(atm);
   __syncthreads();
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned m = __ballot_sync(0xffffffffu, j < nObj);
-  if (j >= nObj) return;
+  const int j0 = blockIdx.x * kAdjObjs + (threadIdx.x & 31);
+  const bool live = j0 < nObj;
+  const bool writer = live && threadIdx.x < 32;
+  const int j = live ? j0 : nObj - 1;
   double r[3] = {st[j], st[nObj + j], st[2 * nObj + j]};
   double v[3] = {st[3 * nObj + j], st[4 * nObj + j], st[5 * nObj + j]};
   const double myBc = bc[j], myAom = aom[j];
-  const bool isA = (j & 1) == 0;
+  const bool isA = (j0 & 1) == 0;
   double best = INFINITY;
-  int arg = 0;
+  int arg = 0, half = 0;
   double acc[3][3];
   for (int s = 1; s <= steps; ++s) {
-    if ((s - 1) % ck == 0) {
+    if ((s - 1) % ck == 0 && writer) {
       const int k = (s - 1) / ck;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -277,44 +371,47 @@ __global__ void __launch_bounds__(128) k_adj_forward(const double *__restrict__ 
         ckpt[((size_t)k * 6 + 3 + c) * nObj + j] = v[c];
       }
     }
-    adjStep(pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
+    adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
     double o[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      o[c] = shflPartner(m, r[c]);
-      o[3 + c] = shflPartner(m, v[c]);
+      o[c] = __shfl_xor_sync(0xffffffffu, r[c], 1);
+      o[3 + c] = __shfl_xor_sync(0xffffffffu, v[c], 1);
     }
-    double dr[3], t;
-    const double d2 = isA ? pairMiss(r, v, o, o + 3, dt, dr, t) : pairMiss(o, o + 3, r, v, dt, dr, t);
+    double dr[3], tt;
+    const double d2 = isA ? pairMiss(r, v, o, o + 3, dt, dr, tt) : pairMiss(o, o + 3, r, v, dt, dr, tt);
     if (d2 < best) {  // NaN never wins
       best = d2;
       arg = s;
     }
   }
-  if (isA) {
+  if (isA && writer) {
     miss[j >> 1] = best;
     argStep[j >> 1] = arg;
   }
 }
 
 // grad[c * nObj + j]: c = 0..5 dL/d(r0, v0), c = 6 dL/dbcInv.  seg: per
-// object ck * 15 doubles, rec[(q * 15 + c) * nObj + j] for step q of the segment.
-__global__ void __launch_bounds__(128) k_adj_backward(const double *__restrict__ bc, const double *__restrict__ aom,
-                                                      int nObj, int steps, int ck, const EphEntry *__restrict__ eph,
-                                                      PropConsts pc, double dt, const double *__restrict__ ckpt,
-                                                      const int *__restrict__ argStep, double *__restrict__ rec,
-                                                      double *__restrict__ grad) {
+// object ck * 15 doubles, rec[(q * 15 + c) * nObj + j] for step q of the
+// segment (written by warp 0, read by every warp of the block).
+__global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
+    const double *__restrict__ bc, const double *__restrict__ aom, int nObj, int steps, int ck,
+    const EphEntry *__restrict__ eph, PropConsts pc, double dt, const double *__restrict__ ckpt,
+    const int *__restrict__ argStep, double *__restrict__ rec, double *__restrict__ grad) {
   __shared__ AtmShared atm;
+  __shared__ AdjExchange<7> ex;
   loadAtm(atm);
   __syncthreads();
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned m = __ballot_sync(0xffffffffu, j < nObj);
-  if (j >= nObj) return;
+  const int j0 = blockIdx.x * kAdjObjs + (threadIdx.x & 31);
+  const bool live = j0 < nObj;
+  const bool writer = live && threadIdx.x < 32;
+  const int j = live ? j0 : nObj - 1;
   const double myBc = bc[j], myAom = aom[j];
-  const bool isA = (j & 1) == 0;
-  const int sStar = argStep[j >> 1];
+  const bool isA = (j0 & 1) == 0;
+  const int sStar = live ? argStep[j >> 1] : 0;
   double lr[3] = {0, 0, 0}, lv[3] = {0, 0, 0}, lbc = 0.0;
   double seedR[3] = {0, 0, 0}, seedV[3] = {0, 0, 0};
+  int half = 0;
   const int nSeg = (steps + ck - 1) / ck;
   for (int seg = nSeg - 1; seg >= 0; --seg) {
     const int s0 = seg * ck, s1 = min(steps, s0 + ck);
@@ -327,33 +424,37 @@ __global__ void __launch_bounds__(128) k_adj_backward(const double *__restrict__
     // recompute the segment, keeping each step's start state and stage accelerations
     for (int s = s0 + 1; s <= s1; ++s) {
       double *q = rec + (size_t)(s - s0 - 1) * 15 * nObj + j;
+      if (writer) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        q[(size_t)c * nObj] = r[c];
-        q[(size_t)(3 + c) * nObj] = v[c];
+        for (int c = 0; c < 3; ++c) {
+          q[(size_t)c * nObj] = r[c];
+          q[(size_t)(3 + c) * nObj] = v[c];
+        }
       }
       double acc[3][3];
-      adjStep(pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
+      adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
+      if (writer) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) q[(size_t)(6 + 3 * a + c) * nObj] = acc[a][c];
+          for (int c = 0; c < 3; ++c) q[(size_t)(6 + 3 * a + c) * nObj] = acc[a][c];
+      }
       // the pair's argmin step is inside this segment: seed from the states after step s
       const bool atStar = s == sStar;
-      if (__any_sync(m, atStar)) {
+      if (__any_sync(0xffffffffu, atStar)) {
         double o[6];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          o[c] = shflPartner(m, r[c]);
-          o[3 + c] = shflPartner(m, v[c]);
+          o[c] = __shfl_xor_sync(0xffffffffu, r[c], 1);
+          o[3 + c] = __shfl_xor_sync(0xffffffffu, v[c], 1);
         }
         if (atStar) {
-          double dr[3], t;
+          double dr[3], tt;
           if (isA)
-            pairMiss(r, v, o, o + 3, dt, dr, t);
+            pairMiss(r, v, o, o + 3, dt, dr, tt);
           else
-            pairMiss(o, o + 3, r, v, dt, dr, t);
-          const double sign = isA ? 2.0 : -2.0, tv = t - dt;
+            pairMiss(o, o + 3, r, v, dt, dr, tt);
+          const double sign = isA ? 2.0 : -2.0, tv = tt - dt;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             seedR[c] = sign * dr[c];
@@ -362,6 +463,7 @@ __global__ void __launch_bounds__(128) k_adj_backward(const double *__restrict__
         }
       }
     }
+    __syncthreads();  // warp 0's records of the segment are visible to the other warps
     // reverse sweep of the segment
     for (int s = s1; s > s0; --s) {
       if (s == sStar) {
@@ -382,15 +484,18 @@ __global__ void __launch_bounds__(128) k_adj_backward(const double *__restrict__
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int c = 0; c < 3; ++c) acc[a][c] = q[(size_t)(6 + 3 * a + c) * nObj];
-      adjReverseStep(pc.mask, r0, v0, acc, myAom, myBc, eph + 3 * (s - 1), atm, pc, lr, lv, lbc);
+      adjReverseStepWarps(ex, half, pc.mask, r0, v0, acc, myAom, myBc, eph + 3 * (s - 1), atm, pc, lr, lv, lbc);
     }
+    __syncthreads();  // every warp has read the segment's records before warp 0 writes the next segment's
   }
+  if (writer) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    grad[(size_t)c * nObj + j] = lr[c];
-    grad[(size_t)(3 + c) * nObj + j] = lv[c];
+    for (int c = 0; c < 3; ++c) {
+      grad[(size_t)c * nObj + j] = lr[c];
+      grad[(size_t)(3 + c) * nObj + j] = lv[c];
+    }
+    grad[(size_t)6 * nObj + j] = lbc;
   }
-  grad[(size_t)6 * nObj + j] = lbc;
 }
 
 // Synthetic conjunction pairs: A forward tca[p] steps, B = A + (dr, dv), then

@@ -10,9 +10,9 @@
 
 namespace ladds {
 
-// Split precision finds the band without a search: every band edge of the
-// table is a multiple of 5 km, so the band of h in [0, 1000) km is a function
-// of floor(h / 5) (a 200-entry table; 1000 km and above: the last band).
+// The band is found without a search: every band edge of the table is a
+// multiple of 5 km, so the band of h in [0, 1000) km is a function of
+// floor(h / 5) (a 200-entry table; 1000 km and above: the last band).
 constexpr int kAtmBand5 = 201;
 struct AtmShared {
   double h0[kAtmBands], rho0[kAtmBands], H[kAtmBands];
@@ -35,14 +35,16 @@ __device__ __forceinline__ void loadAtmTable(AtmShared &atm, const AtmRow *rows)
   }
 }
 
-// band index: largest k with h0[k] <= h (0 below the table)
+// band index: largest k with h0[k] <= h (0 below the table).  The 5 km table
+// gives it up to the rounding of h / 5 at a band edge (every band is at least
+// 5 km wide), which one comparison with each neighbouring edge corrects: the
+// result equals a search of h0 for every h (NaN: band 0).
 __device__ __forceinline__ int atmBand(const AtmShared &t, double h) {
-  int k = 0;
-#pragma unroll
-  for (int step = 16; step >= 1; step >>= 1) {
-    const int c = k + step;
-    if (c < kAtmBands && h >= t.h0[c]) k = c;
-  }
+  int k = t.band5[min(max((int)(h * 0.2), 0), kAtmBand5 - 1)];
+  if (h < t.h0[k])
+    k = max(k - 1, 0);
+  else if (k + 1 < kAtmBands && h >= t.h0[k + 1])
+    k = k + 1;
   return k;
 }
 // the same in binary32 from the 5 km table (split precision: an altitude

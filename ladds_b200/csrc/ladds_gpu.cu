@@ -2494,7 +2494,7 @@ int ladds_gpu_adjoint_forward(ladds_gpu_ctx *c, const ladds_adjoint_pair *pairs,
   if ((rc = adjEphemeris(c, steps))) return rc;
   CK(cudaEventRecord(c->callStart, c->st));
   if (nObj)
-    k_adj_forward<<<blocksFor(nObj, 128), 128, 0, c->st>>>(A.st, A.bc, A.aom, (int)nObj, steps, checkpointEvery,
+    k_adj_forward<<<blocksFor(nObj, kAdjObjs), kAdjWarps * 32, 0, c->st>>>(A.st, A.bc, A.aom, (int)nObj, steps, checkpointEvery,
                                                            A.eph, c->pc, c->cfg.deltaT, A.ckpt, A.miss, A.arg);
   CK(cudaEventRecord(c->callEnd, c->st));
   CK(cudaGetLastError());
@@ -2533,7 +2533,7 @@ int ladds_gpu_adjoint_backward(ladds_gpu_ctx *c, double *dL_dx0, double *dL_dbc,
   const size_t nObj = 2 * A.nPairs;
   CK(cudaEventRecord(c->callStart, c->st));
   if (nObj)
-    k_adj_backward<<<blocksFor(nObj, 128), 128, 0, c->st>>>(A.bc, A.aom, (int)nObj, A.steps, A.ck, A.eph, c->pc,
+    k_adj_backward<<<blocksFor(nObj, kAdjObjs), kAdjWarps * 32, 0, c->st>>>(A.bc, A.aom, (int)nObj, A.steps, A.ck, A.eph, c->pc,
                                                             c->cfg.deltaT, A.ckpt, A.arg, A.rec, A.grad);
   CK(cudaEventRecord(c->callEnd, c->st));
   CK(cudaGetLastError());
