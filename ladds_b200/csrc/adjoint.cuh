@@ -128,11 +128,13 @@ __device__ __forceinline__ void accelConservativeJvp(uint32_t mask, const double
 __device__ __forceinline__ void accelVjp(uint32_t mask, const double r[3], const double v[3], double aom,
                                          double bcInv, const EphEntry &e, const AtmShared &atm, const double g[3],
                                          double lr[3], double lv[3], double &lbc) {
-  double dc[3];
-  accelConservativeJvp(mask, r, g, aom, e, dc);
-  lr[0] += dc[0];
-  lr[1] += dc[1];
-  lr[2] += dc[2];
+  if (mask & ~kPropDRAG) {
+    double dc[3];
+    accelConservativeJvp(mask, r, g, aom, e, dc);
+    lr[0] += dc[0];
+    lr[1] += dc[1];
+    lr[2] += dc[2];
+  }
   if (mask & kPropDRAG) {
     const double x = r[0], y = r[1], z = r[2];
     const double rn = sqrt(x * x + y * y + z * z);
@@ -143,13 +145,16 @@ __device__ __forceinline__ void accelVjp(uint32_t mask, const double r[3], const
     const double rho = atm.rho0[b] * exp(-(h - atm.h0[b]) / atm.H[b]);
     const double K = -0.5e3 * rho * bcInv;
     const double wg = wx * g[0] + wy * g[1] + wz * g[2];
-    const double c1 = K * wn, c2 = wn > 0.0 ? K * wg / wn : 0.0;
+    // the quotients do not depend on the density: they are formed beside its
+    // exponential instead of after it
+    const double wgw = wn > 0.0 ? wg / wn : 0.0, kq = wn * wg / (atm.H[b] * rn);
+    const double c1 = K * wn, c2 = K * wgw;
     const double qx = c1 * g[0] + c2 * wx, qy = c1 * g[1] + c2 * wy, qz = c1 * g[2] + c2 * wz;
     lv[0] += qx;
     lv[1] += qy;
     lv[2] += qz;
     // w = (vx + W y, vy - W x, vz): M^T q = (-W qy, W qx, 0); K depends on |r| through rho(h)
-    const double kr = -K * wn * wg / (atm.H[b] * rn);
+    const double kr = -K * kq;
     lr[0] += -kOmegaEarth * qy + kr * x;
     lr[1] += kOmegaEarth * qx + kr * y;
     lr[2] += kr * z;
@@ -238,6 +243,49 @@ __device__ __forceinline__ void warpTermSum(AdjExchange<N> &ex, int &half, doubl
   }
   half ^= 1;
 }
+
+// The ephemeris of 16 steps (3 stage entries each) staged in shared memory:
+// the terms' reads of the Sun, the Moon and the rotation angle at every stage
+// would otherwise be L2 reads on the chain right after a block barrier.  The
+// next chunk is loaded into registers while the current one is in use (one
+// 16-byte load per thread and slot), and stored to shared memory at the
+// switch, between two block barriers.  Every thread of the block calls use()
+// with the same arguments (the step sequence is the block's).
+constexpr int kEphChunkSteps = 16;
+static_assert(sizeof(EphEntry) % 16 == 0, "ephemeris entries are staged as 16-byte words");
+constexpr int kEphChunkWords = kEphChunkSteps * 3 * (int)(sizeof(EphEntry) / 16);
+constexpr int kEphSlots = (kEphChunkWords + kAdjWarps * 32 - 1) / (kAdjWarps * 32);
+struct EphStage {
+  uint4 pre[kEphSlots];
+  int cur = -1, ahead = -1;  // chunk in shared memory, chunk in the registers
+
+  // issues the loads of chunk c (steps 16 c + 1 .. 16 c + 16 of the S-step ephemeris)
+  __device__ __forceinline__ void fetch(const EphEntry *__restrict__ eph, int steps, int c) {
+    ahead = c;
+    const int words = c < 0 ? 0 : min(steps - c * kEphChunkSteps, kEphChunkSteps) * 3 * (int)(sizeof(EphEntry) / 16);
+    const uint4 *src = reinterpret_cast<const uint4 *>(eph) + (size_t)max(c, 0) * kEphChunkWords;
+#pragma unroll
+    for (int i = 0; i < kEphSlots; ++i) {
+      const int w = (int)threadIdx.x + i * kAdjWarps * 32;
+      if (w < words) pre[i] = __ldg(src + w);
+    }
+  }
+  // makes chunk c current (its loads issued now if the prefetch guessed
+  // another), then prefetches chunk `next`; returns the chunk's first entry
+  __device__ __forceinline__ void use(uint4 *buf, const EphEntry *__restrict__ eph, int steps, int c, int next) {
+    if (c == cur) return;
+    if (ahead != c) fetch(eph, steps, c);
+    __syncthreads();  // no warp reads the previous chunk any more
+#pragma unroll
+    for (int i = 0; i < kEphSlots; ++i) {
+      const int w = (int)threadIdx.x + i * kAdjWarps * 32;
+      if (w < kEphChunkWords) buf[w] = pre[i];
+    }
+    __syncthreads();
+    cur = c;
+    fetch(eph, steps, next);
+  }
+};
 
 // adjStep with the terms shared out over the block's warps
 template <int N>
@@ -349,8 +397,12 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_forward(
     double *__restrict__ miss, int *__restrict__ argStep) {
   __shared__ AtmShared atm;
   __shared__ AdjExchange<3> ex;
+  __shared__ uint4 ephBuf[kEphChunkWords];
   loadAtm(atm);
   __syncthreads();
+  const EphEntry *ephS = reinterpret_cast<const EphEntry *>(ephBuf);
+  EphStage es;
+  es.fetch(eph, steps, 0);
   const int j0 = blockIdx.x * kAdjObjs + (threadIdx.x & 31);
   const bool live = j0 < nObj;
   const bool writer = live && threadIdx.x < 32;
@@ -371,7 +423,9 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_forward(
         ckpt[((size_t)k * 6 + 3 + c) * nObj + j] = v[c];
       }
     }
-    adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
+    const int chunk = (s - 1) / kEphChunkSteps;
+    es.use(ephBuf, eph, steps, chunk, chunk + 1);
+    adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, ephS + 3 * (s - 1 - chunk * kEphChunkSteps), atm, pc, acc);
     double o[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -400,8 +454,11 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
     const int *__restrict__ argStep, double *__restrict__ rec, double *__restrict__ grad) {
   __shared__ AtmShared atm;
   __shared__ AdjExchange<7> ex;
+  __shared__ uint4 ephBuf[kEphChunkWords];
   loadAtm(atm);
   __syncthreads();
+  const EphEntry *ephS = reinterpret_cast<const EphEntry *>(ephBuf);
+  EphStage es;
   const int j0 = blockIdx.x * kAdjObjs + (threadIdx.x & 31);
   const bool live = j0 < nObj;
   const bool writer = live && threadIdx.x < 32;
@@ -413,8 +470,12 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
   double seedR[3] = {0, 0, 0}, seedV[3] = {0, 0, 0};
   int half = 0;
   const int nSeg = (steps + ck - 1) / ck;
+  // ephemeris chunks: each segment ascending (recompute), then descending
+  // (reverse sweep), then the first chunk of the segment before it
+  if (nSeg > 0) es.fetch(eph, steps, (nSeg - 1) * ck / kEphChunkSteps);
   for (int seg = nSeg - 1; seg >= 0; --seg) {
     const int s0 = seg * ck, s1 = min(steps, s0 + ck);
+    const int cFirst = s0 / kEphChunkSteps, cLast = (s1 - 1) / kEphChunkSteps;
     double r[3], v[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -432,7 +493,10 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
         }
       }
       double acc[3][3];
-      adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, eph + 3 * (s - 1), atm, pc, acc);
+      const int chunk = (s - 1) / kEphChunkSteps;
+      es.use(ephBuf, eph, steps, chunk, chunk < cLast ? chunk + 1 : chunk - 1);
+      adjStepWarps(ex, half, pc.mask, r, v, myAom, myBc, ephS + 3 * (s - 1 - chunk * kEphChunkSteps), atm, pc,
+                   acc);
       if (writer) {
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -464,7 +528,13 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
       }
     }
     __syncthreads();  // warp 0's records of the segment are visible to the other warps
-    // reverse sweep of the segment
+    // reverse sweep of the segment; each step's record is loaded one step ahead
+    double qn[15];
+    {
+      const double *q = rec + (size_t)(s1 - s0 - 1) * 15 * nObj + j;
+#pragma unroll
+      for (int c = 0; c < 15; ++c) qn[c] = q[(size_t)c * nObj];
+    }
     for (int s = s1; s > s0; --s) {
       if (s == sStar) {
 #pragma unroll
@@ -473,18 +543,26 @@ __global__ void __launch_bounds__(kAdjWarps * 32) k_adj_backward(
           lv[c] += seedV[c];
         }
       }
-      const double *q = rec + (size_t)(s - s0 - 1) * 15 * nObj + j;
       double r0[3], v0[3], acc[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        r0[c] = q[(size_t)c * nObj];
-        v0[c] = q[(size_t)(3 + c) * nObj];
+        r0[c] = qn[c];
+        v0[c] = qn[3 + c];
       }
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[a][c] = q[(size_t)(6 + 3 * a + c) * nObj];
-      adjReverseStepWarps(ex, half, pc.mask, r0, v0, acc, myAom, myBc, eph + 3 * (s - 1), atm, pc, lr, lv, lbc);
+        for (int c = 0; c < 3; ++c) acc[a][c] = qn[6 + 3 * a + c];
+      if (s - 1 > s0) {
+        const double *q = rec + (size_t)(s - s0 - 2) * 15 * nObj + j;
+#pragma unroll
+        for (int c = 0; c < 15; ++c) qn[c] = q[(size_t)c * nObj];
+      }
+      const int chunk = (s - 1) / kEphChunkSteps;
+      es.use(ephBuf, eph, steps, chunk,
+             chunk > cFirst ? chunk - 1 : (seg > 0 ? (seg - 1) * ck / kEphChunkSteps : -1));
+      adjReverseStepWarps(ex, half, pc.mask, r0, v0, acc, myAom, myBc, ephS + 3 * (s - 1 - chunk * kEphChunkSteps),
+                          atm, pc, lr, lv, lbc);
     }
     __syncthreads();  // every warp has read the segment's records before warp 0 writes the next segment's
   }
