@@ -16,6 +16,9 @@
 // __ddiv_rn) in the reference's evaluation order, so results are bit-identical
 // to a binary64 CPU evaluation without FMA contraction, NaN path included.
 #pragma once
+#include <algorithm>
+#include <cmath>
+
 #include "../../include/ladds_gpu.h"
 #include "physics.cuh"
 #include "state.cuh"
@@ -183,9 +186,26 @@ __device__ __forceinline__ uint32_t functorPair(const ScanConsts &c, const Obj &
 //   does not: its special-function work competes with the propagation that
 //   runs beside the scan.)
 // NaN (identical velocities: the reference's 0/0 path) keeps the pair.
+// the binary32 constants of mayRecord from the scan's parameters (host):
+// dt, factor; rel = 1 + 4 nearRel + 1e-6; thr = max(evasion cutoff, conjunction
+// threshold); cutoff^2, cutoff; nearBand = cutoff^2 nearRel 1.01.  Computed
+// once per scan instead of per screened pair (each was a conversion from
+// binary64 or a square root); the values are those the screen formed itself.
+inline ScanConsts screenConsts(ScanConsts c) {
+  c.dtF = (float)c.dt;
+  c.factorF = (float)c.factor;
+  const float nr = (float)c.nearRel;
+  c.relF = 1.0f + 4.0f * nr + 1e-6f;
+  c.thrF = std::max(std::sqrt((float)c.evasionSq), std::sqrt((float)c.conjSq));
+  c.cut2F = (float)c.cutoffSq;
+  c.cutF = std::sqrt(c.cut2F);
+  c.nearBandF = c.cut2F * nr * 1.01f;
+  return c;
+}
+
 template <bool FAST = false>
 __device__ __forceinline__ bool mayRecord(const ScanConsts &c, float4 pa, float4 va, float4 pb, float4 vb) {
-  const float dt = (float)c.dt;
+  const float dt = c.dtF;
   const float drx = pa.x - pb.x, dry = pa.y - pb.y, drz = pa.z - pb.z;
   const float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
   const float ox = drx - dvx * dt, oy = dry - dvy * dt, oz = drz - dvz * dt;  // separation at the step start
@@ -201,13 +221,12 @@ __device__ __forceinline__ bool mayRecord(const ScanConsts &c, float4 pa, float4
                      fmaxf(fmaxf(fabsf(vb.x), fabsf(vb.y)), fabsf(vb.z));
   const float sepScale = FAST ? d2 * rsqrtf(d2) + dv2 * rsqrtf(dv2) * dt : sqrtf(d2) + sqrtf(dv2) * dt;
   const float err = 3.5f * (pa.w + pb.w) + 3.5e-7f * vmax * dt + 1e-6f * sepScale + 1e-6f;
-  const float rel = 1.0f + 4.0f * (float)c.nearRel + 1e-6f;
-  const float sep = (va.w + vb.w) * (float)c.factor;
-  const float thr = fmaxf(fmaxf(sep, sqrtf((float)c.evasionSq)), sqrtf((float)c.conjSq)) * rel;
+  const float sep = (va.w + vb.w) * c.factorF;
+  const float thr = fmaxf(sep, c.thrF) * c.relF;
   if (!(dl > thr + err)) return true;  // also NaN
   // near band of the cutoff gate: |d^2 - cutoff^2| <= nearRel cutoff^2
-  const float cut2 = (float)c.cutoffSq, d2err = 2.0f * sqrtf(cut2) * err + 1e-5f * cut2;
-  return fabsf(d2 - cut2) <= cut2 * (float)c.nearRel * 1.01f + d2err;
+  const float d2err = 2.0f * c.cutF * err + 1e-5f * c.cut2F;
+  return fabsf(d2 - c.cut2F) <= c.nearBandF + d2err;
 }
 
 __device__ __forceinline__ uint32_t lowerBound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi, uint32_t v) {

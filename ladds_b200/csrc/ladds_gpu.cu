@@ -623,8 +623,9 @@ inline float prefilterRadius(double cutoff, double nearRel) {
 }
 
 // candidates + evaluation on stream s; records carry *iterPtr + iterOffset
-void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &sc, float cutF, const int64_t *iterPtr,
+void enqueueScanWith(ladds_gpu_ctx *c, cudaStream_t s, const ScanConsts &scIn, float cutF, const int64_t *iterPtr,
                      int64_t iterOffset) {
+  const ScanConsts sc = screenConsts(scIn);
   const DenseBin dense = denseBin(c);
   {
     PhaseScope ps(c, kPhCandidates, s, dense.cells ? 2 : 1);
@@ -1026,6 +1027,14 @@ int ladds_gpu_create(const ladds_gpu_config *f, ladds_gpu_ctx **out) {
   cudaMemset(c->dCandCount, 0, 3 * sizeof(unsigned long long));
   cudaMemset(c->dCandNeed, 0, sizeof(unsigned long long));
   c->evalBlocks = 4 * std::max(prop.multiProcessorCount, 1);
+  // The reach-1 list walk runs beside the propagation and the sort of the next
+  // iteration; at its 40 registers twelve of its CTAs fit an SM, and the extra
+  // resident warps slow the iteration beside them more than they speed the
+  // walk.  A shared-memory carveout of 132 KB (57 % of 228 KB) holds it at ten
+  // CTAs per SM: 10 x (12 KB + 1 KB reserved).
+  if (cudaFuncSetAttribute(k_pair_candidates<LADDS_SCREEN_LISTS, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           57) != cudaSuccess)
+    cudaGetLastError();  // a preference only: without it the walk runs with more CTAs per SM
   rc = ensurePairCapacity(c, f->pairCapacity ? (size_t)f->pairCapacity : (size_t)1 << 16);
   if (!rc) rc = ensureCandCapacity(c, (size_t)1 << 16);
   if (rc) {

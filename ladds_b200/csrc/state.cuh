@@ -53,6 +53,9 @@ struct ScanConsts {
   double evasionSq;   // evasionCutoff * evasionCutoff          (CollisionFunctor.cpp:28)
   double conjSq;      // conjunctionThreshold^2
   double nearRel;
+  // binary32 forms for the screen of the pair scan (mayRecord), derived from the
+  // fields above by screenConsts() before every scan launch
+  float dtF, factorF, relF, thrF, cut2F, cutF, nearBandF;
 };
 
 }  // namespace ladds
