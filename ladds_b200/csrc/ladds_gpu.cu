@@ -476,7 +476,9 @@ void launchPropagate(ladds_gpu_ctx *c, const DevState &s, int n, int nSteps, int
   const int g = blocksFor((size_t)n, b);
   uint32_t *rc = c->rowCounts;
   if (keys && stageable(s)) {  // the per-scan propagation: persistent grid, state staged by bulk copies
-    const int sg = std::max(1, std::min(blocksFor((size_t)n, kStageObjects), c->evalBlocks));
+    // two CTAs per SM: alone the kernel is faster with four, but it runs beside
+    // the previous iteration's pair scan, which the other slots then serve
+    const int sg = std::max(1, std::min(blocksFor((size_t)n, kStageObjects), c->evalBlocks / 2));
     if (c->cfg.precision == LADDS_PRECISION_SPLIT)
       k_propagate_staged<true><<<sg, kStageObjects, 0, c->st>>>(s, n, nSteps, ephBase, c->pc, c->grid, keyOut, rc,
                                                                 arrOut, c->dStatus);
