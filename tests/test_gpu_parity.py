@@ -175,7 +175,8 @@ def test_scan_dense_cells_bitexact(capi, oracle, cell, screen):
 @pytest.mark.parametrize("n,span", [(5000, 6.0), (3000, 40.0), (300, 60.0)])
 def test_cell_order_rows_of_every_length(capi, oracle, n, span):
     """Rows of > 4096, 33-256 and <= 32 objects take different sort paths
-    (global-memory bitonic, shared-memory / multi-slot warp bitonic, one
+    (blocked bitonic: stages inside 4096-element blocks in shared memory, the
+    wider ones in global memory; shared-memory / multi-slot warp bitonic; one
     register per lane); the order must equal the stable sort by key."""
     pop = dense_population(21, n=n, span=span)
     with ctx_for(capi, **DENSE_KW) as ctx:
